@@ -1,0 +1,205 @@
+/*
+ * rg_b200.h -- C ABI of the B200 reionization grid step.
+ *
+ * This library replaces the three grid-step entry points of Meraxes:
+ *
+ *   void find_HII_bubbles(int snapshot, timer_info* timer_total);   src/core/find_HII_bubbles.h:13
+ *   void ComputeTs(int snapshot, timer_info* timer_total);          src/core/ComputeTs.h:15
+ *   void ComputeBrightnessTemperatureBox(int snapshot);             src/core/BrightnessTemperature.h:10
+ *
+ * and the legacy device hooks they dispatch to under USE_CUDA:
+ *
+ *   void _find_HII_bubbles_gpu(const int snapshot, const bool flag_write_validation_output);  src/meraxes_gpu.h:53
+ *   void init_CUDA(void);                                                                        src/meraxes_gpu.h:54
+ *
+ * The reference functions read everything from the global run_globals; these
+ * take it explicitly: an rg_params struct with the run_globals.params fields the
+ * step reads, the snapshot's redshift list, and an rg_grids struct of pointers
+ * with the reion_grids_t layouts (src/meraxes.h:448-681):
+ *
+ *   real inputs   float[N][N][2(N/2+1)]  INDEX_PADDED  (src/core/misc_tools.c:249)
+ *   real outputs  float[N][N][N]         INDEX_REAL    (src/core/misc_tools.c:252)
+ *
+ * All entry points return an int status (RG_OK = 0); nothing aborts or throws
+ * across the ABI (the reference calls ABORT / throws C++ exceptions instead).
+ * Calls on one context are not thread-safe; different contexts are independent.
+ */
+#ifndef RG_B200_H
+#define RG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define RG_OK 0
+#define RG_EINVAL 1        /* bad argument or parameter (checked before any launch) */
+#define RG_ENOMEM 2        /* device or host allocation failed */
+#define RG_ECUDA 3         /* a CUDA runtime call failed (rg_last_error() has the text) */
+#define RG_EUNSUPPORTED 4  /* a feature flag the library does not implement */
+#define RG_ETABLE 5        /* a 21cmFAST table file could not be read */
+#define RG_ENODEV 6        /* no usable CUDA device */
+#define RG_ETIMEDOUT 7     /* a bounded device-side wait gave up */
+
+/* ---- parameters: the run_globals.params / .physics / .units fields the step reads ---- */
+typedef struct rg_params {
+  int ReionGridDim;                 /* N */
+  double BoxSize;                   /* Mpc/h */
+  double Hubble_h, OmegaM, OmegaK, OmegaLambda, OmegaR, BaryonFrac, wLambda;
+  double UnitLength_in_cm, UnitMass_in_g, UnitVelocity_in_cm_per_s;
+  /* find_HII_bubbles (src/core/find_HII_bubbles.c:90-285) */
+  double ReionDeltaRFactor, ReionRBubbleMax, ReionRBubbleMaxRecomb, ReionRBubbleMin;
+  int Flag_EvolvingReionRBubbleMax;
+  int ReionFilterType;              /* 0 real-space top-hat, 1 sharp-k, 2 gaussian */
+  int ReionRtoMFilterType;          /* 0 top-hat, 1 gaussian */
+  int ReionUVBFlag;                 /* 0, 1 or 2 */
+  double ReionEfficiency, ReionNionPhotPerBary, ReionGammaHaloBias, ReionAlphaUV, ReionAlphaUVBH;
+  double ReionSfrTimescale, Y_He;
+  int Flag_IncludeSpinTemp, Flag_IncludeRecombinations, Flag_BHFeedback;
+  /* ComputeTs (src/core/ComputeTs.c:85-1554) */
+  int TsHeatingFilterType, TsNumFilterSteps, Flag_IncludeAGNXray;
+  double ReionMaxHeatingRedshift;
+  double NuXrayThreshold, NuXraySoftCut, NuXrayMax;       /* eV */
+  double SpecIndexXrayGal;
+  /* ComputeBrightnessTemperatureBox */
+  int Flag_IncludePecVelsFor21cm;
+  /* directory holding recfast_LCDM.dat, kappa_*_table.dat, stellar_spectra.dat, x_int_tables/ */
+  const char* TablesForXHeatingDir;
+} rg_params;
+
+/* Fill *p with the values of input/params/defaults.par and the Genesis cosmology/units. */
+int rg_params_default(rg_params* p, int grid_dim, double box_size);
+
+/* ---- grids: reion_grids_t fields (device pointers unless an entry point says "host") ---- */
+typedef struct rg_grids {
+  /* padded real inputs [N][N][2(N/2+1)] */
+  const float* deltax;
+  const float* stars;
+  const float* weighted_sfr;
+  const float* effective_bhm;       /* Flag_BHFeedback */
+  const float* effective_bhar;      /* Flag_BHFeedback */
+  /* real [N]^3 outputs of find_HII_bubbles; z_at_ionization, J_21_at_ionization and
+     temp_kinetic_all_gas persist across snapshots (initialise with rg_init_reion_grids) */
+  float* xH;
+  float* r_bubble;
+  float* z_at_ionization;
+  float* J_21_at_ionization;
+  float* temp_kinetic_all_gas;
+  /* spin temperature state: x_e_box_prev and x_e_box padded, Tk_box and TS_box real */
+  float* x_e_box_prev;
+  float* x_e_box;
+  float* Tk_box;
+  float* TS_box;
+  /* ComputeTs sources, padded: sfr and xray_luminosity of this snapshot, and the
+     histories [n_hist][N][N][2(N/2+1)], slot 0 = this snapshot (reionization.c:2093-2140) */
+  const float* sfr;
+  const float* xray_luminosity;
+  const float* sfr_histories;
+  const float* xray_luminosity_histories;
+  int n_hist;
+  /* brightness temperature output, real [N]^3 */
+  float* delta_T;
+} rg_grids;
+
+/* The snapshot being processed: run_globals.ZZ[] and the snapshot index into it. */
+typedef struct rg_snapshot {
+  int snapshot;
+  int n_snapshots;
+  const double* ZZ;                 /* host array, ZZ[0..n_snapshots) descending redshifts */
+  const double* stored_fcoll;       /* host array [n_snapshots]; ComputeTs writes [snapshot] */
+} rg_snapshot;
+
+/* Global averages the reference stores into reion_grids_t (src/meraxes.h:628-675). */
+typedef struct rg_hii_scalars {
+  double volume_weighted_global_xH;
+  double volume_weighted_global_r_bubble;
+  double volume_weighted_global_weighted_sfr;
+  double volume_weighted_global_effective_bhar;
+  double volume_weighted_global_temp_kinetic_all_gas;
+  double mass_weighted_global_xH;
+  double mass_weighted_global_r_bubble;
+  double mass_weighted_global_temp_kinetic_all_gas;
+  int n_radii;                      /* filter radii processed */
+} rg_hii_scalars;
+
+typedef struct rg_ts_scalars {
+  double volume_ave_J_alpha, volume_ave_xalpha, volume_ave_Xheat, volume_ave_Xion;
+  double volume_ave_TS, volume_ave_TK, volume_ave_xe;
+  double collapse_fraction, x_e_ave;      /* the stored_fcoll[snapshot] and <x_e> of this step */
+  int homogeneous;                        /* 1 when zp >= ReionMaxHeatingRedshift */
+} rg_ts_scalars;
+
+typedef struct rg_context rg_context;
+
+/* Execution modes (rg_set_mode). RG_MODE_FUSED is the default. */
+#define RG_MODE_FUSED 0   /* dead-grid elimination, radius batching, graph replay */
+#define RG_MODE_PLAIN 1   /* one 3-D FFT chain per grid per radius, every reference grid */
+
+/* ---- lifetime; replaces init_CUDA() (src/core/meraxes_gpu.cu:127-194) ---- */
+int rg_create(int device, int grid_dim, rg_context** out);
+int rg_destroy(rg_context* ctx);
+int rg_set_mode(rg_context* ctx, int mode);
+int rg_set_radius_batch(rg_context* ctx, int radii_per_batch);   /* 0 = autotuned */
+/* cudaStream_t to launch on (NULL = the context's own stream). */
+int rg_set_stream(rg_context* ctx, void* stream);
+const char* rg_last_error(const rg_context* ctx);
+const char* rg_status_string(int status);
+
+/* Allocate every device grid a step with these flags needs, owned by ctx. */
+int rg_alloc_grids(rg_context* ctx, const rg_params* p, int n_hist, rg_grids* out);
+/* init_reion_grids() (src/core/reionization.c:504-716) for the device grids. */
+int rg_init_reion_grids(rg_context* ctx, const rg_params* p, const rg_grids* g);
+
+/* ---- the grid step (device pointers, asynchronous on the context stream; scalars
+        are written before return, so these synchronise the stream once) ---- */
+
+/* _find_HII_bubbles (src/core/find_HII_bubbles.c:86-710). */
+int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+                        rg_hii_scalars* out);
+/* _ComputeTs (src/core/ComputeTs.c:85-1554). */
+int rg_compute_Ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+                  rg_ts_scalars* out);
+/* ComputeBrightnessTemperatureBox (src/core/BrightnessTemperature.c:24-549); writes *volume_ave_Tb. */
+int rg_delta_T(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+               double* volume_ave_Tb);
+
+/* Host-buffer forms: g holds HOST pointers (the reion_grids_t arrays as Meraxes keeps
+   them); inputs are copied to the context's device grids, the step runs, outputs are
+   copied back.  These are what the USE_B200 shims of find_HII_bubbles(), ComputeTs()
+   and ComputeBrightnessTemperatureBox() call. */
+int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* host,
+                             rg_hii_scalars* out);
+int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* host,
+                       rg_ts_scalars* out);
+int rg_delta_T_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* host,
+                    double* volume_ave_Tb);
+
+/* ---- per-kernel timing: CUDA events on the launching stream around every launch ---- */
+typedef struct rg_kernel_stat {
+  char name[48];
+  int launches;
+  double ms_total;          /* summed event time */
+  double alg_bytes_total;   /* algorithmic HBM bytes (minimum reads + writes) of those launches */
+} rg_kernel_stat;
+int rg_profile_enable(rg_context* ctx, int on);                  /* clears the counters */
+int rg_profile_read(rg_context* ctx, rg_kernel_stat* out, int max, int* n);
+
+/* ---- building blocks exposed for tests ---- */
+
+/* Forward r2c of one padded grid, normalised by 1/N^3, into an internal spectrum slot;
+   then unnormalised c2r of the slot (optionally filtered at radius R) into a padded grid.
+   filter_type < 0 = no filter.  These mirror one forward plan + filter() + reverse plan. */
+int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in_padded,
+                              float* d_out_padded, double R, int filter_type);
+
+/* Radius schedule of find_HII_bubbles: fills up to max_r radii, returns the count in *n. */
+int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int max_r, int* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RG_B200_H */

@@ -1,0 +1,707 @@
+// The C ABI: context lifetime, parameter validation and the host orchestration of the
+// grid step (find_HII_bubbles, ComputeTs, delta_T).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rg_fft.cuh"
+#include "rg_internal.h"
+
+namespace rg {
+
+int set_error(rg_context* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return status;
+}
+
+Units make_units(const rg_params* p) {
+  Units u;
+  u.UnitTime_in_s = p->UnitLength_in_cm / p->UnitVelocity_in_cm_per_s;
+  u.G = GRAVITY / std::pow(p->UnitLength_in_cm, 3) * p->UnitMass_in_g * std::pow(u.UnitTime_in_s, 2);
+  u.Hubble = HUBBLE * u.UnitTime_in_s;
+  u.RhoCrit = 3 * u.Hubble * u.Hubble / (8 * M_PI * u.G);
+  return u;
+}
+
+double hubble_time_at(const rg_params* p, double z) {
+  // hubble_time() = 1 / (Hubble E(z)), src/core/virial_properties.c:6-20,79-96
+  const Units u = make_units(p);
+  const double opz = 1. + z;
+  const double ez = std::sqrt(p->OmegaM * opz * opz * opz + p->OmegaK * opz * opz + p->OmegaLambda);
+  return 1.0 / (u.Hubble * ez);
+}
+
+double dtdz(const rg_params* p, float zf) {
+  // src/core/XRayHeatingFunctions.c:426-440
+  const double z = zf;
+  const double oml = p->OmegaLambda, omm = p->OmegaM;
+  const double x = std::sqrt(oml / omm) * std::pow(1 + z, -3.0 / 2.0);
+  const double dxdz = std::sqrt(oml / omm) * std::pow(1 + z, -5.0 / 2.0) * (-3.0 / 2.0);
+  const double const1 = 2 * std::sqrt(1 + omm / oml) / (3.0 * HUBBLE * p->Hubble_h);
+  const double numer = dxdz * (1 + x * std::pow(std::pow(x, 2) + 1, -0.5));
+  const double denom = x + std::sqrt(std::pow(x, 2) + 1);
+  return const1 * numer / denom;
+}
+
+double rtom(const rg_params* p, double R) {
+  // RtoM(), src/core/find_HII_bubbles.c:27-46
+  const Units u = make_units(p);
+  if (p->ReionRtoMFilterType == 0) return (4.0 / 3.0) * M_PI * std::pow(R, 3) * (p->OmegaM * u.RhoCrit);
+  return std::pow(2 * M_PI, 1.5) * p->OmegaM * u.RhoCrit * std::pow(R, 3);
+}
+
+float cT_approx(float z) { return (float)(0.58 - 0.006 * ((double)z - 10.0)); }
+
+std::vector<std::pair<double, bool>> radius_schedule(const rg_params* p, double z) {
+  // find_HII_bubbles.c:147-148,256-285,546
+  const double box = p->BoxSize;
+  const int n = p->ReionGridDim;
+  double cell_len_factor = L_FACTOR;
+  if ((box / (double)n) < 1.0) cell_len_factor = 1.0;
+  double rmax;
+  if (p->Flag_EvolvingReionRBubbleMax)
+    rmax = z > 6. ? 25.483241248322766 : 112. * std::pow((1. + z) / 5., -4.4);
+  else
+    rmax = p->Flag_IncludeRecombinations ? p->ReionRBubbleMaxRecomb : p->ReionRBubbleMax;
+  double R = std::fmin(rmax, L_FACTOR * box);
+  std::vector<std::pair<double, bool>> out;
+  bool last = false;
+  while (!last) {
+    if (((R / p->ReionDeltaRFactor) <= (cell_len_factor * box / (double)n)) ||
+        ((R / p->ReionDeltaRFactor) <= p->ReionRBubbleMin)) {
+      last = true;
+      R = cell_len_factor * box / (double)n;
+    }
+    out.emplace_back(R, last);
+    R /= p->ReionDeltaRFactor;
+    if (out.size() > 100000) break;  // guards a ReionDeltaRFactor <= 1 that validation missed
+  }
+  return out;
+}
+
+int twiddles_for(rg_context* ctx, int n, const cf** out) {
+  for (auto& e : ctx->twiddles)
+    if (e.first == n) {
+      *out = e.second;
+      return RG_OK;
+    }
+  std::vector<cf> h(n);
+  for (int k = 0; k < n; ++k) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    h[k] = cf{(float)std::cos(a), (float)std::sin(a)};
+  }
+  cf* d = nullptr;
+  RG_CUDA_TRY(ctx, cudaMalloc((void**)&d, sizeof(cf) * n));
+  RG_CUDA_TRY(ctx, cudaMemcpy(d, h.data(), sizeof(cf) * n, cudaMemcpyHostToDevice));
+  ctx->twiddles.emplace_back(n, d);
+  *out = d;
+  return RG_OK;
+}
+
+void prof_begin(rg_context* ctx, const char* name, cudaStream_t st) {
+  if (!ctx->prof_on) return;
+  auto take = [&]() {
+    cudaEvent_t e;
+    if (!ctx->prof_pool.empty()) {
+      e = ctx->prof_pool.back();
+      ctx->prof_pool.pop_back();
+    } else {
+      cudaEventCreate(&e);
+    }
+    return e;
+  };
+  rg_context::ProfRec r;
+  r.name = name;
+  r.e0 = take();
+  r.e1 = take();
+  r.bytes = 0;
+  cudaEventRecord(r.e0, st);
+  ctx->prof_pending.push_back(r);
+}
+
+void prof_end(rg_context* ctx, double alg_bytes, cudaStream_t st) {
+  if (!ctx->prof_on || ctx->prof_pending.empty()) return;
+  auto& r = ctx->prof_pending.back();
+  r.bytes = alg_bytes;
+  cudaEventRecord(r.e1, st);
+}
+
+void prof_resolve(rg_context* ctx) {
+  for (auto& r : ctx->prof_pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(r.e1) == cudaSuccess) cudaEventElapsedTime(&ms, r.e0, r.e1);
+    rg_kernel_stat* st = nullptr;
+    for (auto& k : ctx->prof_stats)
+      if (r.name == k.name) st = &k;
+    if (!st) {
+      rg_kernel_stat k{};
+      std::snprintf(k.name, sizeof(k.name), "%s", r.name.c_str());
+      ctx->prof_stats.push_back(k);
+      st = &ctx->prof_stats.back();
+    }
+    st->launches += 1;
+    st->ms_total += ms;
+    st->alg_bytes_total += r.bytes;
+    ctx->prof_pool.push_back(r.e0);
+    ctx->prof_pool.push_back(r.e1);
+  }
+  ctx->prof_pending.clear();
+}
+
+static bool supported_n(int n) {
+  static const int ok[] = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512};
+  for (int v : ok)
+    if (v == n) return true;
+  return false;
+}
+
+static int ensure_tables(rg_context* ctx, const rg_params* p) {
+  const std::string dir = p->TablesForXHeatingDir ? p->TablesForXHeatingDir : "";
+  if (ctx->tables.loaded && ctx->tables.dir == dir) return RG_OK;
+  if (dir.empty()) return set_error(ctx, RG_ETABLE, "TablesForXHeatingDir is not set");
+  const std::string e = load_tables(dir, p->ReionNionPhotPerBary, &ctx->tables);
+  if (!e.empty()) return set_error(ctx, RG_ETABLE, e);
+  return RG_OK;
+}
+
+template <typename T>
+static int ensure_dev(rg_context* ctx, T** ptr, size_t* have, size_t need) {
+  if (*ptr && *have >= need) return RG_OK;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * need);
+  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  *have = need;
+  return RG_OK;
+}
+
+static int ensure_spectra(rg_context* ctx, const int* which, int nw) {
+  const size_t n = (size_t)ctx->N;
+  const size_t elems = (n / 2 + 1) * n * n;
+  if (ctx->spec_elems != elems) {
+    for (int g = 0; g < HG_COUNT; ++g) {
+      if (ctx->spec[g]) cudaFree(ctx->spec[g]);
+      if (ctx->work[g]) cudaFree(ctx->work[g]);
+      ctx->spec[g] = ctx->work[g] = nullptr;
+    }
+    ctx->spec_elems = elems;
+  }
+  for (int i = 0; i < nw; ++i) {
+    const int g = which[i];
+    if (!ctx->spec[g]) RG_CUDA_TRY(ctx, cudaMalloc((void**)&ctx->spec[g], sizeof(cf) * elems));
+    if (!ctx->work[g]) RG_CUDA_TRY(ctx, cudaMalloc((void**)&ctx->work[g], sizeof(cf) * elems));
+  }
+  return RG_OK;
+}
+
+static int validate_common(rg_context* ctx, const rg_params* p) {
+  if (!ctx || !p) return RG_EINVAL;
+  if (p->ReionGridDim != ctx->N) return set_error(ctx, RG_EINVAL, "ReionGridDim differs from the context's grid");
+  if (!(p->BoxSize > 0)) return set_error(ctx, RG_EINVAL, "BoxSize must be positive");
+  if (!(p->UnitLength_in_cm > 0) || !(p->UnitMass_in_g > 0) || !(p->UnitVelocity_in_cm_per_s > 0))
+    return set_error(ctx, RG_EINVAL, "units must be positive");
+  return RG_OK;
+}
+
+__global__ void k_fill(float* p, size_t n, float v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+static int fill(rg_context* ctx, float* p, size_t n, float v) {
+  if (!p) return RG_OK;
+  if (v == 0.f) {
+    RG_CUDA_TRY(ctx, cudaMemsetAsync(p, 0, n * sizeof(float), ctx->stream));
+    return RG_OK;
+  }
+  k_fill<<<1184, 256, 0, ctx->stream>>>(p, n, v);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  return RG_OK;
+}
+
+}  // namespace rg
+
+using namespace rg;
+
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+const char* rg_status_string(int s) {
+  switch (s) {
+    case RG_OK: return "ok";
+    case RG_EINVAL: return "invalid argument";
+    case RG_ENOMEM: return "out of memory";
+    case RG_ECUDA: return "CUDA error";
+    case RG_EUNSUPPORTED: return "unsupported feature";
+    case RG_ETABLE: return "table file error";
+    case RG_ENODEV: return "no CUDA device";
+    case RG_ETIMEDOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char* rg_last_error(const rg_context* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int rg_params_default(rg_params* p, int grid_dim, double box_size) {
+  if (!p) return RG_EINVAL;
+  std::memset(p, 0, sizeof(*p));
+  p->ReionGridDim = grid_dim;
+  p->BoxSize = box_size;
+  // Genesis cosmology and units (input/params/simulations/Genesis_L10_N512.par:17-31)
+  p->OmegaM = 0.3121;
+  p->OmegaK = 0.0;
+  p->OmegaLambda = 0.6879;
+  p->OmegaR = 0.0;
+  p->BaryonFrac = 0.15714;
+  p->Hubble_h = 0.6751;
+  p->wLambda = -1.0;
+  p->UnitLength_in_cm = 3.08568e+24;
+  p->UnitMass_in_g = 1.989e+43;
+  p->UnitVelocity_in_cm_per_s = 100000;
+  // input/params/defaults.par:233-282
+  p->ReionDeltaRFactor = 1.1;
+  p->ReionRBubbleMax = 20.34;
+  p->ReionRBubbleMaxRecomb = 33.9;
+  p->ReionRBubbleMin = 0.4068;
+  p->Flag_EvolvingReionRBubbleMax = 1;
+  p->ReionFilterType = 0;
+  p->ReionRtoMFilterType = 0;
+  p->ReionUVBFlag = 1;
+  p->ReionNionPhotPerBary = 4000;
+  p->Y_He = 0.24;
+  // set_ReionEfficiency(), src/core/reionization.c:299-328
+  p->ReionEfficiency = 1.0 / p->BaryonFrac * p->ReionNionPhotPerBary / (1.0 - 0.75 * p->Y_He);
+  p->ReionGammaHaloBias = 2.0;
+  p->ReionAlphaUV = 2.0;
+  p->ReionAlphaUVBH = 2.0;
+  p->ReionSfrTimescale = 0.5;
+  p->TsHeatingFilterType = 1;
+  p->TsNumFilterSteps = 40;
+  p->ReionMaxHeatingRedshift = 30.;
+  p->NuXrayThreshold = 500.;
+  p->NuXraySoftCut = 2000.;
+  p->NuXrayMax = 10000.;
+  p->SpecIndexXrayGal = 1.;
+  return RG_OK;
+}
+
+int rg_create(int device, int grid_dim, rg_context** out) {
+  if (!out) return RG_EINVAL;
+  *out = nullptr;
+  if (!supported_n(grid_dim)) return RG_EUNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return RG_ENODEV;
+  if (device < 0 || device >= ndev) return RG_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return RG_ECUDA;
+  rg_context* ctx = new rg_context();
+  ctx->device = device;
+  ctx->N = grid_dim;
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return RG_ECUDA;
+  }
+  ctx->stream = ctx->own_stream;
+  if (cudaMallocHost((void**)&ctx->h_sums, sizeof(double) * 64) != cudaSuccess ||
+      cudaMalloc((void**)&ctx->d_sums, sizeof(double) * 64) != cudaSuccess) {
+    rg_destroy(ctx);
+    return RG_ENOMEM;
+  }
+  *out = ctx;
+  return RG_OK;
+}
+
+int rg_destroy(rg_context* ctx) {
+  if (!ctx) return RG_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& e : ctx->twiddles) cudaFree(e.second);
+  for (int g = 0; g < HG_COUNT; ++g) {
+    if (ctx->spec[g]) cudaFree(ctx->spec[g]);
+    if (ctx->work[g]) cudaFree(ctx->work[g]);
+  }
+  if (ctx->wtab) cudaFree(ctx->wtab);
+  if (ctx->partials) cudaFree(ctx->partials);
+  if (ctx->d_sums) cudaFree(ctx->d_sums);
+  if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
+  if (ctx->d_radii) cudaFree(ctx->d_radii);
+  for (void* p : ctx->owned) cudaFree(p);
+  prof_resolve(ctx);
+  for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return RG_OK;
+}
+
+int rg_set_mode(rg_context* ctx, int mode) {
+  if (!ctx || (mode != RG_MODE_FUSED && mode != RG_MODE_PLAIN)) return RG_EINVAL;
+  ctx->mode = mode;
+  return RG_OK;
+}
+
+int rg_set_radius_batch(rg_context* ctx, int k) {
+  if (!ctx || k < 0 || k > 64) return RG_EINVAL;
+  ctx->radius_batch = k;
+  return RG_OK;
+}
+
+int rg_set_stream(rg_context* ctx, void* stream) {
+  if (!ctx) return RG_EINVAL;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return RG_OK;
+}
+
+int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int max_r, int* n) {
+  if (!p || !n || p->ReionGridDim <= 0 || !(p->BoxSize > 0) || !(p->ReionDeltaRFactor > 1.0)) return RG_EINVAL;
+  auto s = radius_schedule(p, redshift);
+  *n = (int)s.size();
+  for (int i = 0; i < (int)s.size() && i < max_r && radii; ++i) radii[i] = s[i].first;
+  return RG_OK;
+}
+
+int rg_alloc_grids(rg_context* ctx, const rg_params* p, int n_hist, rg_grids* out) {
+  if (!ctx || !p || !out) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  const size_t n = (size_t)ctx->N;
+  const size_t npad = n * n * 2 * (n / 2 + 1), nreal = n * n * n;
+  std::memset(out, 0, sizeof(*out));
+  auto A = [&](size_t elems, float** dst) -> int {
+    void* q = nullptr;
+    if (cudaMalloc(&q, elems * sizeof(float)) != cudaSuccess)
+      return set_error(ctx, RG_ENOMEM, "cudaMalloc failed in rg_alloc_grids");
+    ctx->owned.push_back(q);
+    *dst = (float*)q;
+    return RG_OK;
+  };
+  float* t = nullptr;
+#define RG_ALLOC(field, elems)            \
+  do {                                    \
+    if ((rc = A((elems), &t))) return rc; \
+    out->field = t;                       \
+  } while (0)
+  RG_ALLOC(deltax, npad);
+  RG_ALLOC(stars, npad);
+  RG_ALLOC(weighted_sfr, npad);
+  if (p->Flag_BHFeedback) {
+    RG_ALLOC(effective_bhm, npad);
+    RG_ALLOC(effective_bhar, npad);
+  }
+  RG_ALLOC(xH, nreal);
+  RG_ALLOC(r_bubble, nreal);
+  RG_ALLOC(z_at_ionization, nreal);
+  RG_ALLOC(J_21_at_ionization, nreal);
+  RG_ALLOC(temp_kinetic_all_gas, nreal);
+  RG_ALLOC(delta_T, nreal);
+  if (p->Flag_IncludeSpinTemp) {
+    RG_ALLOC(x_e_box_prev, npad);
+    RG_ALLOC(x_e_box, npad);
+    RG_ALLOC(Tk_box, nreal);
+    RG_ALLOC(TS_box, nreal);
+    RG_ALLOC(sfr, npad);
+    RG_ALLOC(xray_luminosity, npad);
+    if (n_hist > 0) {
+      RG_ALLOC(sfr_histories, npad * (size_t)n_hist);
+      RG_ALLOC(xray_luminosity_histories, npad * (size_t)n_hist);
+    }
+    out->n_hist = n_hist;
+  }
+#undef RG_ALLOC
+  return RG_OK;
+}
+
+int rg_init_reion_grids(rg_context* ctx, const rg_params* p, const rg_grids* g) {
+  if (!ctx || !p || !g) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  const size_t n = (size_t)ctx->N;
+  const size_t npad = n * n * 2 * (n / 2 + 1), nreal = n * n * n;
+  // src/core/reionization.c:557-595
+  if ((rc = fill(ctx, g->xH, nreal, 1.f))) return rc;
+  if ((rc = fill(ctx, g->z_at_ionization, nreal, -1.f))) return rc;
+  if ((rc = fill(ctx, g->r_bubble, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->temp_kinetic_all_gas, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->J_21_at_ionization, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->delta_T, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->Tk_box, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->TS_box, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->x_e_box_prev, npad, 0.f))) return rc;
+  if ((rc = fill(ctx, g->x_e_box, npad, 0.f))) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+                        rg_hii_scalars* out) {
+  if (!ctx || !p || !s || !g || !out || !s->ZZ) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return set_error(ctx, RG_EINVAL, "snapshot out of range");
+  if (p->Flag_IncludeRecombinations)
+    return set_error(ctx, RG_EUNSUPPORTED, "Flag_IncludeRecombinations=1 (MHR00 recombination tables) is not implemented");
+  if (p->ReionFilterType < 0 || p->ReionFilterType > 2)
+    return set_error(ctx, RG_EINVAL, "ReionFilterType must be 0, 1 or 2");
+  if (p->ReionRtoMFilterType < 0 || p->ReionRtoMFilterType > 1)
+    return set_error(ctx, RG_EINVAL, "ReionRtoMFilterType must be 0 or 1");
+  if (!(p->ReionDeltaRFactor > 1.0)) return set_error(ctx, RG_EINVAL, "ReionDeltaRFactor must exceed 1");
+  if (!g->deltax || !g->stars || !g->weighted_sfr || !g->xH || !g->r_bubble || !g->z_at_ionization ||
+      !g->J_21_at_ionization || !g->temp_kinetic_all_gas)
+    return set_error(ctx, RG_EINVAL, "missing grid pointer");
+  const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
+  if (spin && (!g->x_e_box || !g->Tk_box)) return set_error(ctx, RG_EINVAL, "spin temperature needs x_e_box and Tk_box");
+  if (bh && (!g->effective_bhm || !g->effective_bhar)) return set_error(ctx, RG_EINVAL, "BH feedback needs bhm/bhar grids");
+  if ((rc = ensure_tables(ctx, p))) return rc;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+
+  const int N = ctx->N;
+  const double redshift = s->ZZ[s->snapshot];
+  const double box_size = p->BoxSize;
+  const double pixel_volume = std::pow(box_size / (double)N, 3);
+  const Units u = make_units(p);
+  const double sfr_timescale = p->ReionSfrTimescale * hubble_time_at(p, redshift);
+  const double tk_d = T_RECFAST(ctx->tables, (float)redshift);
+  if (tk_d < 0) return set_error(ctx, RG_ETABLE, "T_RECFAST called beyond its table");
+  HiiConst c;
+  c.redshift = (float)redshift;
+  c.TK = (float)tk_d;
+  c.cT_ad = cT_approx((float)redshift);
+  c.uvb = p->ReionUVBFlag;
+  c.spin = spin;
+  c.bh = bh;
+
+  // grids to transform: the ones the barrier test reads.  weighted_sfr (and effective_bhar)
+  // feed only Gamma12 on the recombination branch, so their filtered fields are dead here;
+  // the plain mode transforms them anyway, as the reference does.
+  int act[HG_COUNT];
+  int na = 0;
+  act[na++] = HG_DELTAX;
+  act[na++] = HG_STARS;
+  if (spin) act[na++] = HG_XE;
+  if (bh) act[na++] = HG_BHM;
+  int nplain = na;
+  if (ctx->mode == RG_MODE_PLAIN) act[nplain++] = HG_WSFR;
+  if ((rc = ensure_spectra(ctx, act, nplain))) return rc;
+
+  const float* srcs[HG_COUNT] = {nullptr};
+  cf* specs[HG_COUNT] = {nullptr};
+  cf* works[HG_COUNT] = {nullptr};
+  for (int i = 0; i < nplain; ++i) {
+    const int gg = act[i];
+    srcs[i] = gg == HG_DELTAX ? g->deltax
+            : gg == HG_STARS  ? g->stars
+            : gg == HG_XE     ? g->x_e_box
+            : gg == HG_BHM    ? g->effective_bhm
+                              : g->weighted_sfr;
+    specs[i] = ctx->spec[gg];
+    works[i] = ctx->work[gg];
+  }
+  const double n3 = std::pow((double)N, 3);
+  if ((rc = hii_forward(ctx, N, srcs, specs, nplain, 1.0 / n3, st))) return rc;
+
+  // radius schedule and window table
+  auto sched = radius_schedule(p, redshift);
+  const int nr = (int)sched.size();
+  const int n2max = 3 * (N / 2) * (N / 2);
+  std::vector<double> radii(nr);
+  for (int i = 0; i < nr; ++i) radii[i] = sched[i].first;
+  if ((rc = ensure_dev(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
+  if ((rc = ensure_dev(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
+  if ((rc = hii_window_table(ctx, N, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st))) return rc;
+
+  // r_bubble is only written on the recombination branch: zero it once
+  RG_CUDA_TRY(ctx, cudaMemsetAsync(g->r_bubble, 0, sizeof(float) * (size_t)N * N * N, st));
+
+  // partial-sum buffer for the closing pass
+  const size_t nblocks_max = (size_t)N * N;  // >= grid of the test kernel
+  if ((rc = ensure_dev(ctx, &ctx->partials, &ctx->partials_elems, nblocks_max * HII_NSUM))) return rc;
+
+  HiiState hs;
+  hs.xH = g->xH;
+  hs.z_in = g->z_at_ionization;
+  hs.J21 = g->J_21_at_ionization;
+  hs.temp = g->temp_kinetic_all_gas;
+  hs.Tk_box = spin ? g->Tk_box : nullptr;
+  hs.deltax_unf = g->deltax;
+  hs.wsfr = g->weighted_sfr;
+  hs.bhar = bh ? g->effective_bhar : nullptr;
+  hs.partials = ctx->partials;
+
+  cf* pairs[4] = {ctx->work[HG_DELTAX], ctx->work[HG_STARS], nullptr, nullptr};
+  int npairs = 1;
+  if (spin) {
+    pairs[2] = ctx->work[HG_XE];
+    pairs[3] = bh ? ctx->work[HG_BHM] : nullptr;
+    npairs = 2;
+  } else if (bh) {
+    pairs[2] = ctx->work[HG_BHM];
+    npairs = 2;
+  }
+
+  int nblocks = 0;
+  for (int i = 0; i < nr; ++i) {
+    const double R = sched[i].first;
+    const bool last = sched[i].second;
+    const double M_mean = rtom(p, R);
+    const double R_cubed = R * R * R;
+    // find_HII_bubbles.c:430-442
+    double Gamma_R_prefactor = (1.0 + redshift) * (1.0 + redshift) * R * p->UnitLength_in_cm / pixel_volume *
+                               std::pow(p->UnitLength_in_cm, -3.);
+    Gamma_R_prefactor *= (p->UnitMass_in_g / u.UnitTime_in_s) / PROTONMASS * p->ReionNionPhotPerBary;
+    HiiRadius r;
+    r.J_aux = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
+                      p->ReionAlphaUV);
+    r.J_aux_bh = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
+                         p->ReionAlphaUVBH);
+    r.fcoll_pref = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R_cubed;
+    r.last = last;
+    r.first = (i == 0);
+    r.wtab_row = last ? -1 : i;
+    const float* wrow = last ? nullptr : ctx->wtab + (size_t)i * (n2max + 1);
+    if ((rc = hii_inverse_xy(ctx, N, specs, works, nplain, wrow, st))) return rc;
+    if ((rc = hii_inverse_z_test(ctx, N, pairs, npairs, r, c, hs, last, st, &nblocks))) return rc;
+  }
+  if ((rc = hii_reduce_partials(ctx, ctx->partials, nblocks, HII_NSUM, ctx->d_sums, st))) return rc;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * HII_NSUM, cudaMemcpyDeviceToHost, st));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  prof_resolve(ctx);
+
+  const double* S = ctx->h_sums;
+  const double mass_weight = S[8];
+  out->volume_weighted_global_xH = S[0] / n3;
+  out->volume_weighted_global_r_bubble = S[1] / n3;
+  out->volume_weighted_global_weighted_sfr = S[2] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
+  out->volume_weighted_global_effective_bhar =
+      S[3] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
+  out->volume_weighted_global_temp_kinetic_all_gas = S[4] / n3;
+  out->mass_weighted_global_xH = S[5] / mass_weight;
+  out->mass_weighted_global_r_bubble = S[6] / mass_weight;
+  out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
+  out->n_radii = nr;
+  return RG_OK;
+}
+
+static int copy_grid(rg_context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  if (!dst || !src) return RG_OK;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream));
+  return RG_OK;
+}
+
+static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
+  const bool need_spin = p->Flag_IncludeSpinTemp != 0;
+  const bool need_bh = p->Flag_BHFeedback != 0;
+  if (ctx->dev_grids_ready) {
+    const bool has_spin = ctx->dev_grids.Tk_box != nullptr;
+    const bool has_bh = ctx->dev_grids.effective_bhm != nullptr;
+    if ((!need_spin || has_spin) && (!need_bh || has_bh) && ctx->dev_grids_nhist >= n_hist) return RG_OK;
+    for (void* q : ctx->owned) cudaFree(q);
+    ctx->owned.clear();
+    ctx->dev_grids_ready = false;
+  }
+  int rc = rg_alloc_grids(ctx, p, n_hist, &ctx->dev_grids);
+  if (rc) return rc;
+  ctx->dev_grids_ready = true;
+  ctx->dev_grids_nhist = n_hist;
+  return RG_OK;
+}
+
+int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* h,
+                             rg_hii_scalars* out) {
+  if (!ctx || !p || !s || !h || !out) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  if ((rc = ensure_dev_grids(ctx, p, 0))) return rc;
+  const rg_grids& d = ctx->dev_grids;
+  const size_t n = (size_t)ctx->N;
+  const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float), br = n * n * n * sizeof(float);
+  const auto H2D = cudaMemcpyHostToDevice;
+  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D))) return rc;
+  if ((rc = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D))) return rc;
+  if ((rc = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D))) return rc;
+  if ((rc = copy_grid(ctx, d.temp_kinetic_all_gas, h->temp_kinetic_all_gas, br, H2D))) return rc;
+  if (p->Flag_IncludeSpinTemp) {
+    if ((rc = copy_grid(ctx, d.x_e_box, h->x_e_box, bp, H2D))) return rc;
+    if ((rc = copy_grid(ctx, d.Tk_box, h->Tk_box, br, H2D))) return rc;
+  }
+  if (p->Flag_BHFeedback) {
+    if ((rc = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D))) return rc;
+    if ((rc = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D))) return rc;
+  }
+  if ((rc = rg_find_HII_bubbles(ctx, p, s, &d, out))) return rc;
+  const auto D2H = cudaMemcpyDeviceToHost;
+  if ((rc = copy_grid(ctx, h->xH, d.xH, br, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->r_bubble, d.r_bubble, br, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H))) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R,
+                              int filter_type) {
+  if (!ctx || !p || !d_in || !d_out) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  if (filter_type > 2) return set_error(ctx, RG_EINVAL, "filter_type must be <= 2");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int N = ctx->N;
+  const int which[1] = {HG_DELTAX};
+  if ((rc = ensure_spectra(ctx, which, 1))) return rc;
+  const float* srcs[1] = {d_in};
+  cf* specs[1] = {ctx->spec[HG_DELTAX]};
+  if ((rc = hii_forward(ctx, N, srcs, specs, 1, 1.0 / std::pow((double)N, 3), st))) return rc;
+  const float* wrow = nullptr;
+  if (filter_type >= 0) {
+    const int n2max = 3 * (N / 2) * (N / 2);
+    if ((rc = ensure_dev(ctx, &ctx->d_radii, &ctx->d_radii_elems, 1))) return rc;
+    RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, &R, sizeof(double), cudaMemcpyHostToDevice, st));
+    if ((rc = ensure_dev(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)(n2max + 1)))) return rc;
+    if ((rc = hii_window_table(ctx, N, p->BoxSize, ctx->d_radii, 1, filter_type, ctx->wtab, n2max, st))) return rc;
+    wrow = ctx->wtab;
+  }
+  if ((rc = debug_inverse_to_padded(ctx, N, ctx->spec[HG_DELTAX], ctx->work[HG_DELTAX], wrow, d_out, st))) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return RG_OK;
+}
+
+int rg_profile_enable(rg_context* ctx, int on) {
+  if (!ctx) return RG_EINVAL;
+  prof_resolve(ctx);
+  ctx->prof_on = on != 0;
+  ctx->prof_stats.clear();
+  return RG_OK;
+}
+
+int rg_profile_read(rg_context* ctx, rg_kernel_stat* out, int max, int* n) {
+  if (!ctx || !n) return RG_EINVAL;
+  cudaStreamSynchronize(ctx->stream);
+  prof_resolve(ctx);
+  *n = (int)ctx->prof_stats.size();
+  for (int i = 0; i < *n && i < max && out; ++i) out[i] = ctx->prof_stats[i];
+  return RG_OK;
+}
+
+int rg_compute_Ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_ts_scalars* out) {
+  (void)p; (void)s; (void)g; (void)out;
+  return set_error(ctx, RG_EUNSUPPORTED, "rg_compute_Ts is not built yet");
+}
+
+int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* h,
+                       rg_ts_scalars* out) {
+  (void)p; (void)s; (void)h; (void)out;
+  return set_error(ctx, RG_EUNSUPPORTED, "rg_compute_Ts_host is not built yet");
+}
+
+}  // extern "C"

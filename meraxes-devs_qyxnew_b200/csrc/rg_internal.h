@@ -1,0 +1,171 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rg_b200.h"
+#include "rg_tables.h"
+
+namespace rg {
+
+// physical constants of the reference (src/meraxes.h:21-67, src/core/reionization.h:10-44)
+constexpr double GRAVITY = 6.672e-8;
+constexpr double SOLAR_MASS = 1.989e33;
+constexpr double SOLAR_LUM = 3.826e33;
+constexpr double BOLTZMANN = 1.3806e-16;
+constexpr double SPEED_OF_LIGHT = 2.9979e10;
+constexpr double PLANCK = 6.6262e-27;
+constexpr double PROTONMASS = 1.6726e-24;
+constexpr double HUBBLE = 3.2407789e-18;
+constexpr double SEC_PER_MEGAYEAR = 3.155e13;
+constexpr double SEC_PER_YEAR = 3.155e7;
+constexpr double MPC = 3.086e24;
+constexpr double XRAY_LUMINOSITY_UNIT = 1.0e40;
+constexpr double TCMB = 2.728;
+constexpr double NU_over_EV = 1.60217646e-12 / PLANCK;
+constexpr double NUIONIZATION = 13.60 * NU_over_EV;
+constexpr double HeI_NUIONIZATION = 24.59 * NU_over_EV;
+constexpr double HeII_NUIONIZATION = NUIONIZATION * 4;
+constexpr double NU_LA = 10.2 * NU_over_EV;
+constexpr double T_RE = 1e4;
+constexpr float REL_TOL = 1e-5f;
+constexpr float ABS_TOL = 1e-8f;
+constexpr double SIGMA_HI = 6.3e-18;
+constexpr double TINY = 1e-30;
+constexpr double L_FACTOR = 0.620350491;
+constexpr float MAX_TK = 5e4f;
+constexpr float MIN_TK = 0.1f;
+constexpr double FRACT_FLOAT_ERR = 1e-7;
+constexpr double CLUMPING_FACTOR = 2.0;
+constexpr double T21 = 0.0628;
+constexpr double A10_HYPERFINE = 2.85e-15;
+constexpr double R_XLy_MAX = 500.0;
+constexpr int x_int_NXHII = 14;
+constexpr int x_int_NENERGY = 258;
+constexpr int NSPEC_MAX = 23;
+constexpr int RECFAST_NPTS = 501;
+constexpr int KAPPA_10_NPTS = 27;
+constexpr int KAPPA_10_elec_NPTS = 20;
+constexpr int KAPPA_10_pH_NPTS = 17;
+
+struct cf;
+
+// Derived unit quantities, set_units() (src/core/init.c:203-225).
+struct Units {
+  double UnitTime_in_s, Hubble, G, RhoCrit;
+};
+Units make_units(const rg_params* p);
+double hubble_time_at(const rg_params* p, double z);
+double dtdz(const rg_params* p, float z);
+double rtom(const rg_params* p, double R);
+float cT_approx(float z);
+
+// Radius schedule of the excursion-set loop.
+std::vector<std::pair<double, bool>> radius_schedule(const rg_params* p, double z);
+
+// Status helpers
+int set_error(rg_context* ctx, int status, const std::string& msg);
+#define RG_CUDA_TRY(ctx, call)                                                        \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return ::rg::set_error((ctx), RG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Grids processed by the fused HII pipeline.
+enum HiiGrid { HG_DELTAX = 0, HG_STARS = 1, HG_XE = 2, HG_BHM = 3, HG_WSFR = 4, HG_COUNT = 5 };
+
+// Per-radius constants of the barrier test (find_HII_bubbles.c:427-442).
+struct HiiRadius {
+  double fcoll_pref;
+  float J_aux, J_aux_bh;
+  int last;
+  int first;
+  int wtab_row;        // row of the window table, -1 = unfiltered
+};
+
+struct HiiConst {
+  float redshift, TK, cT_ad;
+  int uvb, spin, bh;
+};
+
+constexpr int HII_NSUM = 9;   // final-pass sums
+
+// Launchers implemented in rg_hii.cu (dispatch on N at run time).
+int hii_forward(rg_context* ctx, int n, const float* const* d_real_padded, cf* const* d_spec, int ngrids,
+                double scale, cudaStream_t st);
+int hii_window_table(rg_context* ctx, int n, double box, const double* radii, int nr, int ftype, float* d_wtab,
+                     int n2max, cudaStream_t st);
+int hii_inverse_xy(rg_context* ctx, int n, cf* const* d_spec, cf* const* d_work, int ngrids, const float* d_wrow,
+                   cudaStream_t st);
+struct HiiState {
+  float* xH;
+  float* z_in;
+  float* J21;
+  float* temp;
+  const float* Tk_box;
+  const float* deltax_unf;   // padded
+  const float* wsfr;         // padded
+  const float* bhar;         // padded, may be null
+  double* partials;          // [nblocks][HII_NSUM]
+};
+int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int npairs, const HiiRadius& r, const HiiConst& c,
+                       const HiiState& s, bool final_pass, cudaStream_t st, int* nblocks_out);
+int hii_reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out,
+                        cudaStream_t st);
+int debug_inverse_to_padded(rg_context* ctx, int n, cf* d_spec, cf* d_work, const float* d_wrow, float* d_out,
+                            cudaStream_t st);
+int twiddles_for(rg_context* ctx, int n, const cf** out);
+
+// Per-kernel event timing (active when ctx->prof_on).  prof_begin records a start event on
+// the stream; prof_end records the stop event and the launch's algorithmic bytes.
+void prof_begin(rg_context* ctx, const char* name, cudaStream_t st);
+void prof_end(rg_context* ctx, double alg_bytes, cudaStream_t st);
+void prof_resolve(rg_context* ctx);   // after a stream sync: fold finished events into the stats
+
+}  // namespace rg
+
+// The opaque context.
+struct rg_context {
+  int device = 0;
+  int N = 0;
+  int mode = RG_MODE_FUSED;
+  int radius_batch = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  // twiddle tables keyed by transform length
+  std::vector<std::pair<int, rg::cf*>> twiddles;
+  // unfiltered spectra and per-radius work buffers (complex, [N/2+1][N][N])
+  rg::cf* spec[rg::HG_COUNT] = {nullptr};
+  rg::cf* work[rg::HG_COUNT] = {nullptr};
+  size_t spec_elems = 0;
+  float* wtab = nullptr;         // window table [nR][n2max+1]
+  size_t wtab_elems = 0;
+  double* partials = nullptr;
+  size_t partials_elems = 0;
+  double* d_sums = nullptr;      // reduced sums
+  double* h_sums = nullptr;      // pinned host copy
+  // device grids owned by the context (rg_alloc_grids / host entry points)
+  std::vector<void*> owned;
+  rg_grids dev_grids{};
+  bool dev_grids_ready = false;
+  int dev_grids_nhist = 0;
+  // host coefficient engine tables, loaded on first use from TablesForXHeatingDir
+  rg::Tables tables;
+  double* d_radii = nullptr;     // device copy of the radius list
+  size_t d_radii_elems = 0;
+  // profiling
+  bool prof_on = false;
+  struct ProfRec {
+    std::string name;
+    cudaEvent_t e0, e1;
+    double bytes;
+  };
+  std::vector<ProfRec> prof_pending;
+  std::vector<cudaEvent_t> prof_pool;
+  std::vector<rg_kernel_stat> prof_stats;
+};

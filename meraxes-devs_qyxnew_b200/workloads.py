@@ -1,0 +1,155 @@
+"""Seeded synthetic inputs for the reionization grid step.
+
+Meraxes builds its source grids from galaxies (``construct_baryon_grids``,
+src/core/reionization.c:2025) and reads the density grid from N-body files
+(src/core/read_grids.c).  Neither is available here, so these generators make
+grids with the same layouts, units and value ranges:
+
+* ``deltax``  : lognormal density contrast ``exp(g - sigma^2/2) - 1`` where ``g``
+  is a Gaussian random field with P(k) ~ k^-2 and a Gaussian cut-off at half the
+  Nyquist wavenumber, normalised to sigma = 0.8;
+* ``stars``   : 1e7 Msun x (1+deltax)^2 x LN(0, 0.5), zeroed in a seeded 80% of
+  the cells, in internal mass units (1e10 Msun/h per cell);
+* ``sfr``     : stars x 1e-8 /yr x LN(0, 0.3), internal mass per internal time;
+  also used as ``weighted_sfr``;
+* ``xray``    : LXrayGal (3.16e40 erg/s per Msun/yr) x SFR, in units of 1e40 erg/s
+  (XRAY_LUMINOSITY_UNIT, src/meraxes.h:36).
+
+Real grids use the FFTW in-place padded layout ``[N][N][2(N/2+1)]``
+(``INDEX_PADDED``, src/core/misc_tools.c:249) with zeros in the padding.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+# cgs constants, src/meraxes.h:21-37
+SOLAR_MASS = 1.989e33
+SEC_PER_YEAR = 3.155e7
+
+# Genesis cosmology and units (input/params/simulations/Genesis_L10_N512.par:17-31)
+COSMO = dict(OmegaM=0.3121, OmegaK=0.0, OmegaLambda=0.6879, OmegaR=0.0,
+             BaryonFrac=0.15714, Hubble_h=0.6751, wLambda=-1.0)
+UNITS = dict(UnitLength_in_cm=3.08568e24, UnitMass_in_g=1.989e43,
+             UnitVelocity_in_cm_per_s=1.0e5)
+
+
+def padded_shape(n: int) -> tuple[int, int, int]:
+    return (n, n, 2 * (n // 2 + 1))
+
+
+def to_padded(real: np.ndarray) -> np.ndarray:
+    """Embed an [N][N][N] array in the FFTW in-place padded layout (float32)."""
+    n = real.shape[0]
+    out = np.zeros(padded_shape(n), dtype=np.float32)
+    out[:, :, :n] = real
+    return out
+
+
+def from_padded(pad: np.ndarray) -> np.ndarray:
+    n = pad.shape[0]
+    return pad[:, :, :n]
+
+
+def gaussian_field(n: int, box: float, rng: np.random.Generator, sigma: float = 0.8) -> np.ndarray:
+    """Gaussian random field with P(k) ~ k^-2 exp(-k^2 / (2 kc^2)), kc = 0.5 k_Nyq."""
+    white = rng.standard_normal((n, n, n))
+    wk = np.fft.rfftn(white)
+    kf = 2.0 * np.pi / box
+    kx = np.fft.fftfreq(n, d=1.0 / n) * kf
+    kz = np.fft.rfftfreq(n, d=1.0 / n) * kf
+    k2 = kx[:, None, None] ** 2 + kx[None, :, None] ** 2 + kz[None, None, :] ** 2
+    k_nyq = np.pi * n / box
+    kc = 0.5 * k_nyq
+    with np.errstate(divide="ignore"):
+        pk = np.where(k2 > 0, 1.0 / k2, 0.0) * np.exp(-k2 / (2.0 * kc * kc))
+    g = np.fft.irfftn(wk * np.sqrt(pk), s=(n, n, n))
+    g -= g.mean()
+    g *= sigma / g.std()
+    return g
+
+
+@dataclasses.dataclass
+class SourceGrids:
+    n: int
+    box: float
+    deltax: np.ndarray        # padded float32
+    stars: np.ndarray         # padded float32, internal mass units
+    sfr: np.ndarray           # padded float32, internal mass / internal time
+    xray: np.ndarray          # padded float32, 1e40 erg/s
+
+
+def make_sources(n: int, box: float, seed: int, source_scale: float = 1.0) -> SourceGrids:
+    rng = np.random.default_rng(seed)
+    sigma = 0.8
+    g = gaussian_field(n, box, rng, sigma)
+    deltax = np.exp(g - 0.5 * sigma * sigma) - 1.0
+    h = COSMO["Hubble_h"]
+    unit_time_s = UNITS["UnitLength_in_cm"] / UNITS["UnitVelocity_in_cm_per_s"]
+    msun_internal = h / 1e10                      # 1 Msun in 1e10 Msun/h
+    stars = 1e7 * msun_internal * (1.0 + deltax) ** 2 * rng.lognormal(0.0, 0.5, size=deltax.shape)
+    stars *= source_scale
+    stars[rng.random(deltax.shape) < 0.8] = 0.0
+    per_year_internal = unit_time_s / SEC_PER_YEAR   # 1/yr -> 1/internal time
+    sfr = stars * 1e-8 * per_year_internal * rng.lognormal(0.0, 0.3, size=deltax.shape)
+    # SFR in Msun/yr, then L_X in 1e40 erg/s
+    sfr_msun_yr = sfr * UNITS["UnitMass_in_g"] / SOLAR_MASS / per_year_internal
+    xray = 3.16e40 * sfr_msun_yr / 1.0e40
+    return SourceGrids(n=n, box=box, deltax=to_padded(deltax), stars=to_padded(stars),
+                       sfr=to_padded(sfr), xray=to_padded(xray))
+
+
+def snapshot_redshifts(z_target: float, z_first: float = 40.0, n_before: int = 60,
+                       dlog: float | None = None) -> tuple[np.ndarray, int]:
+    """Descending snapshot redshift list ending at ``z_target`` (index returned).
+
+    Snapshots are uniform in log(1+z) from ``z_first`` down to ``z_target``,
+    the way N-body snapshot lists usually are.  Two extra later snapshots
+    follow so the list looks like a run in progress.
+    """
+    if dlog is None:
+        dlog = (math.log1p(z_first) - math.log1p(z_target)) / n_before
+    zz = [math.expm1(math.log1p(z_target) + dlog * (n_before - i)) for i in range(n_before + 1)]
+    zz += [math.expm1(math.log1p(z_target) - dlog * j) for j in (1, 2)]
+    return np.asarray(zz, dtype=np.float64), n_before
+
+
+# ReionEfficiency as set_ReionEfficiency() (src/core/reionization.c:299-328) makes it
+# from the defaults: 1/BaryonFrac * ReionNionPhotPerBary / (1 - 0.75 Y_He).
+DEFAULT_REION_EFFICIENCY = 1.0 / 0.15714 * 4000.0 / (1.0 - 0.75 * 0.24)
+
+
+@dataclasses.dataclass
+class GridConfig:
+    """One workload configuration: grid size, box, redshift and reionization params."""
+    name: str
+    n: int
+    box: float               # Mpc/h
+    z: float
+    filter_type: int = 0
+    delta_r_factor: float = 1.1
+    r_bubble_max: float = 50.0
+    r_bubble_min: float = 0.4068
+    evolving_rmax: int = 0
+    efficiency: float = 1.0
+    uvb_flag: int = 1
+    spin_temp: int = 0
+    ts_filter_type: int = 1
+    ts_steps: int = 40
+    seed: int = 1809
+    source_scale: float = 1.0
+
+
+CONFIGS = {
+    # plain find_HII_bubbles, 64^3, 64 Mpc/h, z=8, tophat, R from 50 Mpc/h, f=1.1, eff=1.0
+    "c0_64": GridConfig("c0_64", 64, 64.0, 8.0, seed=1809),
+    # the same generators at 256^3, 250 Mpc/h, z=7
+    "c1_256": GridConfig("c1_256", 256, 250.0, 7.0, seed=1810),
+    # ComputeTs + delta_T at 128^3, 128 Mpc/h, z=15, 40 shells, sharp-k heating filter
+    "c3_128": GridConfig("c3_128", 128, 128.0, 15.0, spin_temp=1, seed=1812),
+    # full step at 512^3, 500 Mpc/h, z=8, R0 = 0.62*L (about 60 radii), then Ts and delta_T
+    "c4_512": GridConfig("c4_512", 512, 500.0, 8.0, r_bubble_max=1000.0, spin_temp=1, seed=1813),
+}

@@ -1,0 +1,73 @@
+"""Shared helpers for the tests: device grids from numpy, and oracle set-up."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+import rg_b200 as rg
+import reion_oracle as ro
+import tables
+
+
+def oracle_params(p: rg.rg_params) -> ro.Params:
+    """The oracle's Params from the ABI struct (same field names)."""
+    kw = {}
+    for f in ro.Params.__dataclass_fields__:
+        if hasattr(p, f):
+            kw[f] = getattr(p, f)
+    return ro.Params(**kw)
+
+
+_RECFAST = None
+
+
+def install_recfast():
+    global _RECFAST
+    if _RECFAST is None:
+        _RECFAST = tables.Recfast(tables.default_tables_dir())
+        ro.set_recfast(_RECFAST.T)
+    return _RECFAST
+
+
+class DeviceGrids:
+    """torch CUDA buffers for an rg_grids struct."""
+
+    def __init__(self, n: int, spin: bool = False, bh: bool = False):
+        import torch
+        self.torch = torch
+        self.n = n
+        npad = n * n * 2 * (n // 2 + 1)
+        nreal = n ** 3
+        dev = "cuda:0"
+        z = lambda k: torch.zeros(k, dtype=torch.float32, device=dev)
+        self.t = {
+            "deltax": z(npad), "stars": z(npad), "weighted_sfr": z(npad),
+            "xH": z(nreal), "r_bubble": z(nreal), "z_at_ionization": torch.full((nreal,), -1.0, device=dev),
+            "J_21_at_ionization": z(nreal), "temp_kinetic_all_gas": z(nreal), "delta_T": z(nreal),
+        }
+        if spin:
+            self.t.update({"x_e_box": z(npad), "x_e_box_prev": z(npad), "Tk_box": z(nreal), "TS_box": z(nreal),
+                           "sfr": z(npad), "xray_luminosity": z(npad)})
+        if bh:
+            self.t.update({"effective_bhm": z(npad), "effective_bhar": z(npad)})
+        self.g = rg.rg_grids()
+        for k, v in self.t.items():
+            setattr(self.g, k, v.data_ptr())
+
+    def put(self, name: str, arr: np.ndarray):
+        self.t[name].copy_(self.torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32).ravel()))
+
+    def get(self, name: str, real: bool = True) -> np.ndarray:
+        a = self.t[name].cpu().numpy()
+        n = self.n
+        if a.size == n ** 3:
+            return a.reshape(n, n, n)
+        return a.reshape(n, n, 2 * (n // 2 + 1))
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
