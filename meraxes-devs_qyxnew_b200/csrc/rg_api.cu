@@ -534,16 +534,11 @@ int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* 
   hs.bhar = bh ? g->effective_bhar : nullptr;
   hs.partials = ctx->partials;
 
-  cf* pairs[4] = {ctx->work[HG_DELTAX], ctx->work[HG_STARS], nullptr, nullptr};
-  int npairs = 1;
-  if (spin) {
-    pairs[2] = ctx->work[HG_XE];
-    pairs[3] = bh ? ctx->work[HG_BHM] : nullptr;
-    npairs = 2;
-  } else if (bh) {
-    pairs[2] = ctx->work[HG_BHM];
-    npairs = 2;
-  }
+  // grids of the test, in the order the kernel reads them: deltax, stars, [x_e], [bhm]
+  cf* tgrids[4] = {ctx->work[HG_DELTAX], ctx->work[HG_STARS], nullptr, nullptr};
+  int ntest = 2;
+  if (spin) tgrids[ntest++] = ctx->work[HG_XE];
+  if (bh) tgrids[ntest++] = ctx->work[HG_BHM];
 
   int nblocks = 0;
   for (int i = 0; i < nr; ++i) {
@@ -566,7 +561,7 @@ int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* 
     r.wtab_row = last ? -1 : i;
     const float* wrow = last ? nullptr : ctx->wtab + (size_t)i * (n2max + 1);
     if ((rc = hii_inverse_xy(ctx, N, specs, works, nplain, wrow, st))) return rc;
-    if ((rc = hii_inverse_z_test(ctx, N, pairs, npairs, r, c, hs, last, st, &nblocks))) return rc;
+    if ((rc = hii_inverse_z_test(ctx, N, tgrids, ntest, r, c, hs, last, st, &nblocks))) return rc;
   }
   if ((rc = hii_reduce_partials(ctx, ctx->partials, nblocks, HII_NSUM, ctx->d_sums, st))) return rc;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * HII_NSUM, cudaMemcpyDeviceToHost, st));

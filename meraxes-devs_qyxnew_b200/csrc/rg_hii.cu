@@ -5,8 +5,9 @@
 // forward chain is z-r2c (rows of the padded real grid, two rows per complex FFT) ->
 // y-c2c (contiguous lines) -> x-c2c (lines of stride N, scaled by 1/N^3).  The inverse
 // chain per radius is x-c2c with the window applied on load -> y-c2c -> z-c2r fused
-// with the aliasing clamp and the barrier test (two grids per complex FFT), so the
-// per-cell state (xH, z_at_ionization, J_21, temperature) is touched once per radius.
+// with the aliasing clamp and the barrier test (two neighbouring rows of a grid per complex
+// FFT), so the per-cell state (xH, z_at_ionization, J_21, temperature) is touched once per
+// radius.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -195,34 +196,45 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Fill a [N][B+1] tile with Z = A + iB, the full-length spectrum of two real lines whose
-// Hermitian halves A, B sit at src_a/src_b[k * pitch_k + b] for k in [0, N/2].  The DC and
+// Fill a [N][B/2+1] tile with Z_q = X(y0+2q) + i X(y0+2q+1): the full-length spectra of two
+// neighbouring rows of ONE grid, whose Hermitian halves sit at src[base + k*pitch_k + y - y0]
+// for k in [0, N/2].  After the inverse FFT the real part is row y0+2q and the imaginary part
+// row y0+2q+1.  Rows of one grid share a magnitude scale, so the rounding each row picks up
+// from its partner stays at the level of a separate transform (pairing two different grids,
+// e.g. deltax ~ 1 with stars ~ 1e-3, would leak deltax-sized rounding into stars).  The DC and
 // Nyquist terms keep only their real parts, as a c2r transform does.
 template <int N, int B>
-__device__ __forceinline__ void build_pair_tile(cf* buf, const cf* __restrict__ ga, const cf* __restrict__ gb,
-                                                size_t base, size_t pitch_k) {
-  constexpr int PS = B + 1;
+__device__ __forceinline__ void build_rowpair_tile(cf* buf, const cf* __restrict__ g, size_t base, size_t pitch_k) {
+  constexpr int P = B / 2;
+  constexpr int PS = P + 1;
   constexpr int NZ = N / 2 + 1;
-  for (int t = threadIdx.x; t < NZ * B; t += NT) {
-    const int b = t % B, k = t / B;
-    const size_t idx = base + (size_t)k * pitch_k + b;
-    const cf a = ga[idx];
-    const cf bb = gb != nullptr ? gb[idx] : cf{0.f, 0.f};
+  for (int t = threadIdx.x; t < NZ * P; t += NT) {
+    const int q = t % P, k = t / P;
+    const size_t idx = base + (size_t)k * pitch_k + 2 * q;
+    const cf a = g[idx];
+    const cf bb = g[idx + 1];
     if (k == 0 || k == N / 2) {
-      buf[k * PS + b] = cf{a.x, bb.x};
+      buf[k * PS + q] = cf{a.x, bb.x};
     } else {
-      buf[k * PS + b] = cf{a.x - bb.y, a.y + bb.x};
-      buf[(N - k) * PS + b] = cf{a.x + bb.y, bb.x - a.y};
+      buf[k * PS + q] = cf{a.x - bb.y, a.y + bb.x};
+      buf[(N - k) * PS + q] = cf{a.x + bb.y, bb.x - a.y};
     }
   }
 }
 
-// z: c2r of the (deltax, stars) [and (x_e, bhm)] pairs, then per cell the clamp and barrier
-// test of find_HII_bubbles.c:373-544; with FINAL also the closing pass of :577-645.
-template <int N, int B, int NPAIR, bool FINAL>
+// value of row y0+b at z in a row-pair tile
+template <int B>
+__device__ __forceinline__ float rowpair_val(const cf* tile, int z, int b) {
+  const cf v = tile[z * (B / 2 + 1) + (b >> 1)];
+  return (b & 1) ? v.y : v.x;
+}
+
+// z: c2r of each grid (deltax, stars [, x_e] [, effective_bhm]), then per cell the clamp and
+// barrier test of find_HII_bubbles.c:373-544; with FINAL also the closing pass of :577-645.
+template <int N, int B, int NG, bool FINAL>
 __global__ void __launch_bounds__(NT) k_inv_z_test(SrcPack works, const cf* __restrict__ g_tw, HiiRadius r,
                                                    HiiConst c, HiiState s) {
-  constexpr int PS = B + 1;
+  constexpr int TS = N * (B / 2 + 1);   // one grid's tile
   constexpr int PADW = 2 * (N / 2 + 1);
   extern __shared__ cf smem[];
   cf* s_tw = smem;
@@ -232,12 +244,12 @@ __global__ void __launch_bounds__(NT) k_inv_z_test(SrcPack works, const cf* __re
   const int y0 = blockIdx.x * B;
   load_twiddles<N, NT>(s_tw, g_tw);
 #pragma unroll
-  for (int pr = 0; pr < NPAIR; ++pr)
-    build_pair_tile<N, B>(tiles + pr * N * PS, static_cast<const cf*>(works.p[2 * pr]),
-                          static_cast<const cf*>(works.p[2 * pr + 1]), (size_t)x * N + y0, (size_t)N * N);
+  for (int gi = 0; gi < NG; ++gi)
+    build_rowpair_tile<N, B>(tiles + gi * TS, static_cast<const cf*>(works.p[gi]), (size_t)x * N + y0,
+                             (size_t)N * N);
   __syncthreads();
 #pragma unroll
-  for (int pr = 0; pr < NPAIR; ++pr) tile_fft<N, true, B, NT>(tiles + pr * N * PS, s_tw);
+  for (int gi = 0; gi < NG; ++gi) tile_fft<N, true, B / 2, NT>(tiles + gi * TS, s_tw);
 
   double acc[HII_NSUM];
 #pragma unroll
@@ -248,21 +260,19 @@ __global__ void __launch_bounds__(NT) k_inv_z_test(SrcPack works, const cf* __re
     const int y = y0 + b;
     const size_t ir = ((size_t)x * N + y) * N + z;
     const size_t ip = ((size_t)x * N + y) * PADW + z;
-    const cf v0 = tiles[z * PS + b];
-    const float dx = fmaxf(v0.x, -1.f + REL_TOL);
-    float st = fmaxf(v0.y, 0.f);
+    const float dx = fmaxf(rowpair_val<B>(tiles, z, b), -1.f + REL_TOL);
+    float st = fmaxf(rowpair_val<B>(tiles + TS, z, b), 0.f);
     if (st < ABS_TOL) st = 0.f;
-    // second pair: (x_e, effective_bhm) with spin temperature, (effective_bhm, -) without
+    // grids 2.. : x_e with spin temperature, then effective_bhm with BH feedback
     float xe = 0.f, bhm = 0.f;
-    if (NPAIR > 1) {
-      const cf v1 = tiles[N * PS + z * PS + b];
+    if (NG > 2) {
       if (c.spin) {
-        xe = fmaxf(v1.x, 0.f);
+        xe = fmaxf(rowpair_val<B>(tiles + 2 * TS, z, b), 0.f);
         if (xe < ABS_TOL) xe = 0.f;
         xe = fminf(xe, 0.999f);
       }
       if (c.bh) {
-        bhm = fmaxf(c.spin ? v1.y : v1.x, 0.f);
+        bhm = fmaxf(rowpair_val<B>(tiles + (c.spin ? 3 : 2) * TS, z, b), 0.f);
         if (bhm < ABS_TOL) bhm = 0.f;
       }
     }
@@ -487,7 +497,7 @@ static int inverse_xy_n(rg_context* ctx, cf* const* d_spec, cf* const* d_work, i
   return RG_OK;
 }
 
-template <int N, int NPAIR, bool FINAL>
+template <int N, int NG, bool FINAL>
 static int inverse_z_test_n3(rg_context* ctx, cf* const* d_work, const HiiRadius& r, const HiiConst& c,
                              const HiiState& s, cudaStream_t st, int* nblocks) {
   const cf* tw;
@@ -495,20 +505,18 @@ static int inverse_z_test_n3(rg_context* ctx, cf* const* d_work, const HiiRadius
   if (rc) return rc;
   constexpr int B = Tiles<N>::BT;
   SrcPack w{};
-  for (int g = 0; g < 2 * NPAIR; ++g) w.p[g] = d_work[g];
-  const size_t sm = sizeof(cf) * (N + NPAIR * N * (B + 1));
-  RG_CUDA_TRY(ctx, prep(k_inv_z_test<N, B, NPAIR, FINAL>, sm));
+  for (int g = 0; g < NG; ++g) w.p[g] = d_work[g];
+  const size_t sm = sizeof(cf) * (N + NG * N * (B / 2 + 1));
+  RG_CUDA_TRY(ctx, prep(k_inv_z_test<N, B, NG, FINAL>, sm));
   const dim3 grid(N / B, N);
   // algorithmic bytes: the Hermitian halves read once, xH read (after the first radius)
   // and written, z_at_ionization read; the closing pass adds deltax, weighted_sfr,
   // effective_bhar, Tk_box reads and the temperature read + write.
   const double n3 = (double)N * N * N, nzc = (double)(N / 2 + 1) * N * N;
-  int ngrid = 0;
-  for (int g = 0; g < 2 * NPAIR; ++g) ngrid += d_work[g] != nullptr;
-  double bytes = ngrid * 8.0 * nzc + (r.first ? 0.0 : 4.0 * n3) + 4.0 * n3 + 4.0 * n3;
+  double bytes = NG * 8.0 * nzc + (r.first ? 0.0 : 4.0 * n3) + 4.0 * n3 + 4.0 * n3;
   if (FINAL) bytes += 4.0 * n3 * (2 + (s.bhar != nullptr) + (s.Tk_box != nullptr) + 2);
   prof_begin(ctx, FINAL ? "inv_z_c2r_test_final" : "inv_z_c2r_test", st);
-  k_inv_z_test<N, B, NPAIR, FINAL><<<grid, NT, sm, st>>>(w, tw, r, c, s);
+  k_inv_z_test<N, B, NG, FINAL><<<grid, NT, sm, st>>>(w, tw, r, c, s);
   prof_end(ctx, bytes, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   if (nblocks) *nblocks = (int)(grid.x * grid.y);
@@ -516,13 +524,16 @@ static int inverse_z_test_n3(rg_context* ctx, cf* const* d_work, const HiiRadius
 }
 
 template <int N>
-static int inverse_z_test_n(rg_context* ctx, cf* const* d_work, int npairs, const HiiRadius& r, const HiiConst& c,
+static int inverse_z_test_n(rg_context* ctx, cf* const* d_work, int ngrids, const HiiRadius& r, const HiiConst& c,
                             const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
-  if (npairs == 1)
-    return fin ? inverse_z_test_n3<N, 1, true>(ctx, d_work, r, c, s, st, nblocks)
-               : inverse_z_test_n3<N, 1, false>(ctx, d_work, r, c, s, st, nblocks);
-  return fin ? inverse_z_test_n3<N, 2, true>(ctx, d_work, r, c, s, st, nblocks)
-             : inverse_z_test_n3<N, 2, false>(ctx, d_work, r, c, s, st, nblocks);
+  if (ngrids == 2)
+    return fin ? inverse_z_test_n3<N, 2, true>(ctx, d_work, r, c, s, st, nblocks)
+               : inverse_z_test_n3<N, 2, false>(ctx, d_work, r, c, s, st, nblocks);
+  if (ngrids == 3)
+    return fin ? inverse_z_test_n3<N, 3, true>(ctx, d_work, r, c, s, st, nblocks)
+               : inverse_z_test_n3<N, 3, false>(ctx, d_work, r, c, s, st, nblocks);
+  return fin ? inverse_z_test_n3<N, 4, true>(ctx, d_work, r, c, s, st, nblocks)
+             : inverse_z_test_n3<N, 4, false>(ctx, d_work, r, c, s, st, nblocks);
 }
 
 template <int N>
@@ -569,9 +580,9 @@ int hii_inverse_xy(rg_context* ctx, int n, cf* const* d_spec, cf* const* d_work,
   RG_DISPATCH_N(n, inverse_xy_n<NN>(ctx, d_spec, d_work, ng, wrow, st));
 }
 
-int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int npairs, const HiiRadius& r, const HiiConst& c,
+int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int ngrids, const HiiRadius& r, const HiiConst& c,
                        const HiiState& s, bool final_pass, cudaStream_t st, int* nblocks_out) {
-  RG_DISPATCH_N(n, inverse_z_test_n<NN>(ctx, d_work, npairs, r, c, s, final_pass, st, nblocks_out));
+  RG_DISPATCH_N(n, inverse_z_test_n<NN>(ctx, d_work, ngrids, r, c, s, final_pass, st, nblocks_out));
 }
 
 int debug_inverse_to_padded(rg_context* ctx, int n, cf* d_spec, cf* d_work, const float* wrow, float* d_out,

@@ -112,7 +112,7 @@ struct HiiState {
   const float* bhar;         // padded, may be null
   double* partials;          // [nblocks][HII_NSUM]
 };
-int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int npairs, const HiiRadius& r, const HiiConst& c,
+int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int ngrids, const HiiRadius& r, const HiiConst& c,
                        const HiiState& s, bool final_pass, cudaStream_t st, int* nblocks_out);
 int hii_reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out,
                         cudaStream_t st);

@@ -66,7 +66,7 @@ def gaussian_field(n: int, box: float, rng: np.random.Generator, sigma: float = 
     kc = 0.5 * k_nyq
     with np.errstate(divide="ignore"):
         pk = np.where(k2 > 0, 1.0 / k2, 0.0) * np.exp(-k2 / (2.0 * kc * kc))
-    g = np.fft.irfftn(wk * np.sqrt(pk), s=(n, n, n))
+    g = np.fft.irfftn(wk * np.sqrt(pk), s=(n, n, n), axes=(0, 1, 2))
     g -= g.mean()
     g *= sigma / g.std()
     return g
