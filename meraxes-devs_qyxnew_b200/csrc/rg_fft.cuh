@@ -1,16 +1,17 @@
-// Shared-memory Stockham FFT building blocks for sm_100a.
+// Register-resident Stockham FFT building blocks for sm_100a.
 //
-// A tile in shared memory holds B independent complex lines of length L.  Element
-// (pos p, line b) lives at buf[p * PS + b] with PS = B + 1: lines are the fast
-// axis, so a warp's accesses during a butterfly stage touch consecutive words, and
-// the odd pitch keeps column-wise fills (threads walking p) at 2-way bank sharing.
+// A line of length N is transformed by T threads.  The transform is the self-sorting
+// Stockham factorisation N = R_0 R_1 ... R_{S-1}: at stage s, butterfly j (0 <= j < N/R_s)
+// reads x[j + r N/R_s] (r < R_s), multiplies by exp(-+2 pi i r (j mod NS) / (NS R_s)) with
+// NS = R_0 ... R_{s-1}, does a radix-R_s DFT in registers and writes its R_s results to
+// (j / NS) NS R_s + (j mod NS) + r NS.  Thread t owns butterflies j = t, t + T, ... at every
+// stage, so it always holds V = N / T values in registers.  Stage 0 reads through a load
+// functor (global memory, or a prologue that builds the input), the last stage writes through
+// a store functor (global memory, or an epilogue); between stages the values cross shared
+// memory once (write, barrier, read).  With the radix plans below that is one exchange for
+// N = 64, 128, 256 and two for N = 96, 192, 512.
 //
-// The transform is the self-sorting Stockham formulation: log_R(L) stages, each
-// reading R elements spaced L/R apart, twiddling, doing a radix-R DFT in registers
-// and writing them to their sorted positions.  Reads of a stage complete (barrier)
-// before its writes, so one buffer suffices.  L must be 2^a 3^b; radices 8, 4, 2
-// and 3 are used, largest first.  Twiddles exp(-2 pi i k / L) come from a table in
-// shared memory that was rounded once from double precision on the host.
+// Twiddles come from a table exp(-2 pi i k / N) in shared memory, rounded once from double.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,21 +19,35 @@
 
 namespace rg {
 
-struct cf {  // complex float, 8 bytes
+struct __align__(8) cf {  // complex float
   float x, y;
 };
 
-__device__ __forceinline__ cf cmk(float a, float b) { return cf{a, b}; }
 __device__ __forceinline__ cf cadd(cf a, cf b) { return cf{a.x + b.x, a.y + b.y}; }
 __device__ __forceinline__ cf csub(cf a, cf b) { return cf{a.x - b.x, a.y - b.y}; }
 __device__ __forceinline__ cf cmul(cf a, cf b) {
   return cf{fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x)};
 }
-__device__ __forceinline__ cf cconj(cf a) { return cf{a.x, -a.y}; }
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>
 __device__ __forceinline__ cf mul_mi(cf a) {
   return INV ? cf{-a.y, a.x} : cf{a.y, -a.x};
+}
+// multiply by exp(-+ 2 pi i m / 16), m in [0, 16)
+template <bool INV, int M>
+__device__ __forceinline__ cf mul_w16(cf a) {
+  constexpr int m = M % 16;
+  if constexpr (m == 0) return a;
+  constexpr float C[4] = {1.0f, 0.92387953251128675613f, 0.70710678118654752440f, 0.38268343236508977173f};
+  // cos and sin of 2 pi m / 16 from the first-quadrant table
+  constexpr int q = m / 4, rr = m % 4;
+  constexpr float c0 = rr == 0 ? 1.0f : C[rr];
+  constexpr float s0 = rr == 0 ? 0.0f : C[4 - rr];
+  constexpr float c = q == 0 ? c0 : q == 1 ? -s0 : q == 2 ? -c0 : s0;
+  constexpr float s = q == 0 ? s0 : q == 1 ? c0 : q == 2 ? -s0 : -c0;
+  // forward: (c - i s), inverse: (c + i s)
+  const float sg = INV ? s : -s;
+  return cf{a.x * c - a.y * sg, a.x * sg + a.y * c};
 }
 
 // ---------------------------------------------------------------------------
@@ -64,16 +79,41 @@ __device__ __forceinline__ void dft8(cf* v) {
   cf o[4] = {v[1], v[3], v[5], v[7]};
   dft4<INV>(e);
   dft4<INV>(o);
-  // o[k] *= W8^k
-  o[1] = INV ? cf{h * (o[1].x - o[1].y), h * (o[1].x + o[1].y)}
-             : cf{h * (o[1].x + o[1].y), h * (o[1].y - o[1].x)};
+  o[1] = INV ? cf{h * (o[1].x - o[1].y), h * (o[1].x + o[1].y)} : cf{h * (o[1].x + o[1].y), h * (o[1].y - o[1].x)};
   o[2] = mul_mi<INV>(o[2]);
-  o[3] = INV ? cf{-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y)}
-             : cf{h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y)};
+  o[3] = INV ? cf{-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y)} : cf{h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y)};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     v[k] = cadd(e[k], o[k]);
     v[k + 4] = csub(e[k], o[k]);
+  }
+}
+
+// 16 = 4 x 4: DFT4 over n1 of x[4 n1 + n2], twiddle W16^(n2 k1), DFT4 over n2 -> X[k1 + 4 k2]
+template <bool INV>
+__device__ __forceinline__ void dft16(cf* v) {
+  cf a[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) a[n2][n1] = v[4 * n1 + n2];
+    dft4<INV>(a[n2]);
+  }
+  a[1][1] = mul_w16<INV, 1>(a[1][1]);
+  a[1][2] = mul_w16<INV, 2>(a[1][2]);
+  a[1][3] = mul_w16<INV, 3>(a[1][3]);
+  a[2][1] = mul_w16<INV, 2>(a[2][1]);
+  a[2][2] = mul_w16<INV, 4>(a[2][2]);
+  a[2][3] = mul_w16<INV, 6>(a[2][3]);
+  a[3][1] = mul_w16<INV, 3>(a[3][1]);
+  a[3][2] = mul_w16<INV, 6>(a[3][2]);
+  a[3][3] = mul_w16<INV, 9>(a[3][3]);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    cf b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    dft4<INV>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
   }
 }
 
@@ -83,8 +123,7 @@ __device__ __forceinline__ void dft3(cf* v) {
   cf t = cadd(v[1], v[2]);
   cf d = csub(v[1], v[2]);
   cf m = cf{v[0].x - 0.5f * t.x, v[0].y - 0.5f * t.y};
-  // forward: y1 = m - i s d, y2 = m + i s d ; inverse swaps the signs
-  cf isd = cf{-s * d.y, s * d.x};  // i * s * d
+  cf isd = cf{-s * d.y, s * d.x};  // i s d
   v[0] = cadd(v[0], t);
   if (INV) {
     v[1] = cadd(m, isd);
@@ -98,78 +137,127 @@ __device__ __forceinline__ void dft3(cf* v) {
 template <int R, bool INV>
 __device__ __forceinline__ void dft_small(cf* v) {
   if constexpr (R == 2) dft2<INV>(v);
+  else if constexpr (R == 3) dft3<INV>(v);
   else if constexpr (R == 4) dft4<INV>(v);
   else if constexpr (R == 8) dft8<INV>(v);
-  else if constexpr (R == 3) dft3<INV>(v);
+  else if constexpr (R == 16) dft16<INV>(v);
 }
 
-template <int REM>
-struct PickRadix {
-  static constexpr int value = (REM % 8 == 0) ? 8 : (REM % 4 == 0) ? 4 : (REM % 2 == 0) ? 2 : 3;
-  static_assert(REM % value == 0, "transform length must be 2^a 3^b");
+// ---------------------------------------------------------------------------
+// radix plans: stages R[0..S) and threads per line T (T divides every N / R[s])
+
+template <int N>
+struct Plan;
+#define RG_PLAN(n, t, ...)                       \
+  template <>                                    \
+  struct Plan<n> {                               \
+    static constexpr int T = t;                  \
+    static constexpr int R[] = {__VA_ARGS__};    \
+    static constexpr int S = sizeof(R) / sizeof(int); \
+  };
+RG_PLAN(8, 1, 8)
+RG_PLAN(16, 1, 16)
+RG_PLAN(24, 1, 8, 3)
+RG_PLAN(32, 4, 8, 4)
+RG_PLAN(48, 2, 8, 2, 3)
+RG_PLAN(64, 8, 8, 8)
+RG_PLAN(96, 4, 8, 4, 3)
+RG_PLAN(128, 8, 16, 8)
+RG_PLAN(192, 8, 8, 8, 3)
+RG_PLAN(256, 16, 16, 16)
+RG_PLAN(384, 16, 8, 8, 2, 3)
+RG_PLAN(512, 64, 8, 8, 8)
+#undef RG_PLAN
+
+template <int N, int s>
+struct StageNS {
+  static constexpr int value = StageNS<N, s - 1>::value * Plan<N>::R[s - 1];
+};
+template <int N>
+struct StageNS<N, 0> {
+  static constexpr int value = 1;
 };
 
-// One Stockham stage over all B lines of the tile, executed by NT threads.
-template <int L, int R, int NS, bool INV, int B, int NT>
-__device__ __forceinline__ void stockham_stage(cf* buf, const cf* tw) {
-  constexpr int PS = B + 1;
-  constexpr int NBF = (L / R) * B;
-  constexpr int K = (NBF + NT - 1) / NT;
-  cf v[K][R];
+template <int N>
+constexpr int plan_product() {
+  int p = 1;
+  for (int i = 0; i < Plan<N>::S; ++i) p *= Plan<N>::R[i];
+  return p;
+}
+
+// run stage s: fill v from `load(pos)`, twiddle, DFT
+template <int N, int s, bool INV, class Load>
+__device__ __forceinline__ void stage_compute(cf* v, int t, const cf* __restrict__ tw, Load&& load) {
+  constexpr int T = Plan<N>::T;
+  constexpr int R = Plan<N>::R[s];
+  constexpr int NS = StageNS<N, s>::value;
+  constexpr int K = (N / R) / T;
+  static_assert((N / R) % T == 0, "T must divide N/R");
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    const int t = threadIdx.x + k * NT;
-    if (NBF % NT == 0 || t < NBF) {
-      const int b = t % B;
-      const int j = t / B;
+    const int j = t + k * T;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[k][r] = buf[(j + r * (L / R)) * PS + b];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const int t = threadIdx.x + k * NT;
-    if (NBF % NT == 0 || t < NBF) {
-      const int b = t % B;
-      const int j = t / B;
+    for (int r = 0; r < R; ++r) v[k * R + r] = load(j + r * (N / R));
+    if constexpr (NS > 1) {
       const int jm = j % NS;
-      if constexpr (NS > 1) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) {
-          cf w = tw[(r * jm * (L / (NS * R))) % L];
-          if (INV) w.y = -w.y;
-          v[k][r] = cmul(v[k][r], w);
-        }
+      for (int r = 1; r < R; ++r) {
+        cf w = tw[(r * jm * (N / (NS * R))) % N];
+        if (INV) w.y = -w.y;
+        v[k * R + r] = cmul(v[k * R + r], w);
       }
-      dft_small<R, INV>(v[k]);
-      const int idxD = (j / NS) * NS * R + jm;
-#pragma unroll
-      for (int r = 0; r < R; ++r) buf[(idxD + r * NS) * PS + b] = v[k][r];
     }
-  }
-  __syncthreads();
-}
-
-template <int L, int NS, bool INV, int B, int NT>
-__device__ __forceinline__ void fft_stages(cf* buf, const cf* tw) {
-  if constexpr (NS < L) {
-    constexpr int R = PickRadix<L / NS>::value;
-    stockham_stage<L, R, NS, INV, B, NT>(buf, tw);
-    fft_stages<L, NS * R, INV, B, NT>(buf, tw);
+    dft_small<R, INV>(v + k * R);
   }
 }
 
-// In-place FFT of all B lines of a [L][B+1] tile.  Starts and ends with a barrier-clean state.
-template <int L, bool INV, int B, int NT>
-__device__ __forceinline__ void tile_fft(cf* buf, const cf* tw) {
-  fft_stages<L, 1, INV, B, NT>(buf, tw);
+// hand stage s's outputs to `put(pos, value)`
+template <int N, int s, class Put>
+__device__ __forceinline__ void stage_emit(const cf* v, int t, Put&& put) {
+  constexpr int T = Plan<N>::T;
+  constexpr int R = Plan<N>::R[s];
+  constexpr int NS = StageNS<N, s>::value;
+  constexpr int K = (N / R) / T;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int j = t + k * T;
+    const int idxD = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+    for (int r = 0; r < R; ++r) put(idxD + r * NS, v[k * R + r]);
+  }
 }
 
-// Copy the L-entry twiddle table into shared memory (caller syncs).
-template <int L, int NT>
+template <int N, int s, bool INV, class Addr, class Store>
+__device__ __forceinline__ void stages_from(cf* v, int t, cf* xbuf, Addr&& addr, const cf* tw, Store&& store) {
+  if constexpr (s + 1 < Plan<N>::S) {
+    __syncthreads();  // every thread is done reading xbuf
+    stage_emit<N, s>(v, t, [&](int p, cf x) { xbuf[addr(p)] = x; });
+    __syncthreads();
+    stage_compute<N, s + 1, INV>(v, t, tw, [&](int p) { return xbuf[addr(p)]; });
+    stages_from<N, s + 1, INV>(v, t, xbuf, addr, tw, store);
+  } else {
+    stage_emit<N, s>(v, t, store);
+  }
+}
+
+// Full transform of one line by thread t (0 <= t < Plan<N>::T):
+//   load(p)        -> input element at position p
+//   addr(p)        -> index into xbuf of position p of this thread's line (exchange buffer)
+//   store(p, val)  <- output element at position p
+// Every thread of the block must call it (it contains block barriers when S > 1).
+template <int N, bool INV, class Load, class Addr, class Store>
+__device__ __forceinline__ void line_fft(int t, cf* xbuf, const cf* tw, Load&& load, Addr&& addr, Store&& store) {
+  static_assert(plan_product<N>() == N, "radix plan does not multiply to N");
+  constexpr int V = N / Plan<N>::T;
+  cf v[V];
+  stage_compute<N, 0, INV>(v, t, tw, load);
+  stages_from<N, 0, INV>(v, t, xbuf, addr, tw, store);
+}
+
+// Copy the N-entry twiddle table into shared memory (caller syncs).
+template <int N>
 __device__ __forceinline__ void load_twiddles(cf* s_tw, const cf* __restrict__ g_tw) {
-  for (int i = threadIdx.x; i < L; i += NT) s_tw[i] = g_tw[i];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s_tw[i] = g_tw[i];
 }
 
 }  // namespace rg
