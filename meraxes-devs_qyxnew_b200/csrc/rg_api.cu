@@ -152,14 +152,14 @@ void prof_resolve(rg_context* ctx) {
   ctx->prof_pending.clear();
 }
 
-static bool supported_n(int n) {
+bool supported_n(int n) {
   static const int ok[] = {8, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512};
   for (int v : ok)
     if (v == n) return true;
   return false;
 }
 
-static int ensure_tables(rg_context* ctx, const rg_params* p) {
+int ensure_tables(rg_context* ctx, const rg_params* p) {
   const std::string dir = p->TablesForXHeatingDir ? p->TablesForXHeatingDir : "";
   if (ctx->tables.loaded && ctx->tables.dir == dir) return RG_OK;
   if (dir.empty()) return set_error(ctx, RG_ETABLE, "TablesForXHeatingDir is not set");
@@ -168,38 +168,17 @@ static int ensure_tables(rg_context* ctx, const rg_params* p) {
   return RG_OK;
 }
 
-template <typename T>
-static int ensure_dev(rg_context* ctx, T** ptr, size_t* have, size_t need) {
-  if (*ptr && *have >= need) return RG_OK;
-  if (*ptr) cudaFree(*ptr);
-  *ptr = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * need);
-  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  *have = need;
-  return RG_OK;
+double* ensure_partials(rg_context* ctx, size_t n) {
+  if (ctx->partials && ctx->partials_elems >= n) return ctx->partials;
+  if (ctx->partials) cudaFree(ctx->partials);
+  ctx->partials = nullptr;
+  ctx->partials_elems = 0;
+  if (cudaMalloc((void**)&ctx->partials, sizeof(double) * n) != cudaSuccess) return nullptr;
+  ctx->partials_elems = n;
+  return ctx->partials;
 }
 
-static int ensure_spectra(rg_context* ctx, const int* which, int nw) {
-  const size_t n = (size_t)ctx->N;
-  const size_t elems = (n / 2 + 1) * n * n;
-  if (ctx->spec_elems != elems) {
-    for (int g = 0; g < HG_COUNT; ++g) {
-      if (ctx->spec[g]) cudaFree(ctx->spec[g]);
-      if (ctx->work[g]) cudaFree(ctx->work[g]);
-      ctx->spec[g] = ctx->work[g] = nullptr;
-    }
-    ctx->spec_elems = elems;
-  }
-  for (int i = 0; i < nw; ++i) {
-    const int g = which[i];
-    if (!ctx->spec[g]) RG_CUDA_TRY(ctx, cudaMalloc((void**)&ctx->spec[g], sizeof(cf) * elems));
-    if (!ctx->work[g]) RG_CUDA_TRY(ctx, cudaMalloc((void**)&ctx->work[g], sizeof(cf) * elems));
-  }
-  return RG_OK;
-}
-
-static int validate_common(rg_context* ctx, const rg_params* p) {
+int validate_common(rg_context* ctx, const rg_params* p) {
   if (!ctx || !p) return RG_EINVAL;
   if (p->ReionGridDim != ctx->N) return set_error(ctx, RG_EINVAL, "ReionGridDim differs from the context's grid");
   if (!(p->BoxSize > 0)) return set_error(ctx, RG_EINVAL, "BoxSize must be positive");
@@ -320,10 +299,9 @@ int rg_destroy(rg_context* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->twiddles) cudaFree(e.second);
-  for (int g = 0; g < HG_COUNT; ++g) {
-    if (ctx->spec[g]) cudaFree(ctx->spec[g]);
-    if (ctx->work[g]) cudaFree(ctx->work[g]);
-  }
+  if (ctx->spec) cudaFree(ctx->spec);
+  if (ctx->work) cudaFree(ctx->work);
+  if (ctx->bits) cudaFree(ctx->bits);
   if (ctx->wtab) cudaFree(ctx->wtab);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
@@ -453,134 +431,13 @@ int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* 
   if (!g->deltax || !g->stars || !g->weighted_sfr || !g->xH || !g->r_bubble || !g->z_at_ionization ||
       !g->J_21_at_ionization || !g->temp_kinetic_all_gas)
     return set_error(ctx, RG_EINVAL, "missing grid pointer");
-  const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
-  if (spin && (!g->x_e_box || !g->Tk_box)) return set_error(ctx, RG_EINVAL, "spin temperature needs x_e_box and Tk_box");
-  if (bh && (!g->effective_bhm || !g->effective_bhar)) return set_error(ctx, RG_EINVAL, "BH feedback needs bhm/bhar grids");
+  if (p->Flag_IncludeSpinTemp && (!g->x_e_box || !g->Tk_box))
+    return set_error(ctx, RG_EINVAL, "spin temperature needs x_e_box and Tk_box");
+  if (p->Flag_BHFeedback && (!g->effective_bhm || !g->effective_bhar))
+    return set_error(ctx, RG_EINVAL, "BH feedback needs effective_bhm and effective_bhar");
   if ((rc = ensure_tables(ctx, p))) return rc;
   cudaSetDevice(ctx->device);
-  cudaStream_t st = ctx->stream;
-
-  const int N = ctx->N;
-  const double redshift = s->ZZ[s->snapshot];
-  const double box_size = p->BoxSize;
-  const double pixel_volume = std::pow(box_size / (double)N, 3);
-  const Units u = make_units(p);
-  const double sfr_timescale = p->ReionSfrTimescale * hubble_time_at(p, redshift);
-  const double tk_d = T_RECFAST(ctx->tables, (float)redshift);
-  if (tk_d < 0) return set_error(ctx, RG_ETABLE, "T_RECFAST called beyond its table");
-  HiiConst c;
-  c.redshift = (float)redshift;
-  c.TK = (float)tk_d;
-  c.cT_ad = cT_approx((float)redshift);
-  c.uvb = p->ReionUVBFlag;
-  c.spin = spin;
-  c.bh = bh;
-
-  // grids to transform: the ones the barrier test reads.  weighted_sfr (and effective_bhar)
-  // feed only Gamma12 on the recombination branch, so their filtered fields are dead here;
-  // the plain mode transforms them anyway, as the reference does.
-  int act[HG_COUNT];
-  int na = 0;
-  act[na++] = HG_DELTAX;
-  act[na++] = HG_STARS;
-  if (spin) act[na++] = HG_XE;
-  if (bh) act[na++] = HG_BHM;
-  int nplain = na;
-  if (ctx->mode == RG_MODE_PLAIN) act[nplain++] = HG_WSFR;
-  if ((rc = ensure_spectra(ctx, act, nplain))) return rc;
-
-  const float* srcs[HG_COUNT] = {nullptr};
-  cf* specs[HG_COUNT] = {nullptr};
-  cf* works[HG_COUNT] = {nullptr};
-  for (int i = 0; i < nplain; ++i) {
-    const int gg = act[i];
-    srcs[i] = gg == HG_DELTAX ? g->deltax
-            : gg == HG_STARS  ? g->stars
-            : gg == HG_XE     ? g->x_e_box
-            : gg == HG_BHM    ? g->effective_bhm
-                              : g->weighted_sfr;
-    specs[i] = ctx->spec[gg];
-    works[i] = ctx->work[gg];
-  }
-  const double n3 = std::pow((double)N, 3);
-  if ((rc = hii_forward(ctx, N, srcs, specs, nplain, 1.0 / n3, st))) return rc;
-
-  // radius schedule and window table
-  auto sched = radius_schedule(p, redshift);
-  const int nr = (int)sched.size();
-  const int n2max = 3 * (N / 2) * (N / 2);
-  std::vector<double> radii(nr);
-  for (int i = 0; i < nr; ++i) radii[i] = sched[i].first;
-  if ((rc = ensure_dev(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
-  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
-  if ((rc = ensure_dev(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
-  if ((rc = hii_window_table(ctx, N, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st))) return rc;
-
-  // r_bubble is only written on the recombination branch: zero it once
-  RG_CUDA_TRY(ctx, cudaMemsetAsync(g->r_bubble, 0, sizeof(float) * (size_t)N * N * N, st));
-
-  // partial-sum buffer for the closing pass
-  const size_t nblocks_max = (size_t)N * N;  // >= grid of the test kernel
-  if ((rc = ensure_dev(ctx, &ctx->partials, &ctx->partials_elems, nblocks_max * HII_NSUM))) return rc;
-
-  HiiState hs;
-  hs.xH = g->xH;
-  hs.z_in = g->z_at_ionization;
-  hs.J21 = g->J_21_at_ionization;
-  hs.temp = g->temp_kinetic_all_gas;
-  hs.Tk_box = spin ? g->Tk_box : nullptr;
-  hs.deltax_unf = g->deltax;
-  hs.wsfr = g->weighted_sfr;
-  hs.bhar = bh ? g->effective_bhar : nullptr;
-  hs.partials = ctx->partials;
-
-  // grids of the test, in the order the kernel reads them: deltax, stars, [x_e], [bhm]
-  cf* tgrids[4] = {ctx->work[HG_DELTAX], ctx->work[HG_STARS], nullptr, nullptr};
-  int ntest = 2;
-  if (spin) tgrids[ntest++] = ctx->work[HG_XE];
-  if (bh) tgrids[ntest++] = ctx->work[HG_BHM];
-
-  int nblocks = 0;
-  for (int i = 0; i < nr; ++i) {
-    const double R = sched[i].first;
-    const bool last = sched[i].second;
-    const double M_mean = rtom(p, R);
-    const double R_cubed = R * R * R;
-    // find_HII_bubbles.c:430-442
-    double Gamma_R_prefactor = (1.0 + redshift) * (1.0 + redshift) * R * p->UnitLength_in_cm / pixel_volume *
-                               std::pow(p->UnitLength_in_cm, -3.);
-    Gamma_R_prefactor *= (p->UnitMass_in_g / u.UnitTime_in_s) / PROTONMASS * p->ReionNionPhotPerBary;
-    HiiRadius r;
-    r.J_aux = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
-                      p->ReionAlphaUV);
-    r.J_aux_bh = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
-                         p->ReionAlphaUVBH);
-    r.fcoll_pref = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R_cubed;
-    r.last = last;
-    r.first = (i == 0);
-    r.wtab_row = last ? -1 : i;
-    const float* wrow = last ? nullptr : ctx->wtab + (size_t)i * (n2max + 1);
-    if ((rc = hii_inverse_xy(ctx, N, specs, works, nplain, wrow, st))) return rc;
-    if ((rc = hii_inverse_z_test(ctx, N, tgrids, ntest, r, c, hs, last, st, &nblocks))) return rc;
-  }
-  if ((rc = hii_reduce_partials(ctx, ctx->partials, nblocks, HII_NSUM, ctx->d_sums, st))) return rc;
-  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * HII_NSUM, cudaMemcpyDeviceToHost, st));
-  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  prof_resolve(ctx);
-
-  const double* S = ctx->h_sums;
-  const double mass_weight = S[8];
-  out->volume_weighted_global_xH = S[0] / n3;
-  out->volume_weighted_global_r_bubble = S[1] / n3;
-  out->volume_weighted_global_weighted_sfr = S[2] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
-  out->volume_weighted_global_effective_bhar =
-      S[3] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
-  out->volume_weighted_global_temp_kinetic_all_gas = S[4] / n3;
-  out->mass_weighted_global_xH = S[5] / mass_weight;
-  out->mass_weighted_global_r_bubble = S[6] / mass_weight;
-  out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
-  out->n_radii = nr;
-  return RG_OK;
+  return hii_snapshot(ctx, p, s, g, out);
 }
 
 static int copy_grid(rg_context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
@@ -650,24 +507,8 @@ int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* 
   if (rc) return rc;
   if (filter_type > 2) return set_error(ctx, RG_EINVAL, "filter_type must be <= 2");
   cudaSetDevice(ctx->device);
-  cudaStream_t st = ctx->stream;
-  const int N = ctx->N;
-  const int which[1] = {HG_DELTAX};
-  if ((rc = ensure_spectra(ctx, which, 1))) return rc;
-  const float* srcs[1] = {d_in};
-  cf* specs[1] = {ctx->spec[HG_DELTAX]};
-  if ((rc = hii_forward(ctx, N, srcs, specs, 1, 1.0 / std::pow((double)N, 3), st))) return rc;
-  const float* wrow = nullptr;
-  if (filter_type >= 0) {
-    const int n2max = 3 * (N / 2) * (N / 2);
-    if ((rc = ensure_dev(ctx, &ctx->d_radii, &ctx->d_radii_elems, 1))) return rc;
-    RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, &R, sizeof(double), cudaMemcpyHostToDevice, st));
-    if ((rc = ensure_dev(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)(n2max + 1)))) return rc;
-    if ((rc = hii_window_table(ctx, N, p->BoxSize, ctx->d_radii, 1, filter_type, ctx->wtab, n2max, st))) return rc;
-    wrow = ctx->wtab;
-  }
-  if ((rc = debug_inverse_to_padded(ctx, N, ctx->spec[HG_DELTAX], ctx->work[HG_DELTAX], wrow, d_out, st))) return rc;
-  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if ((rc = debug_roundtrip(ctx, p, d_in, d_out, R, filter_type))) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }
 

@@ -59,10 +59,6 @@ int delta_T_launch(rg_context* ctx, int n, const float* xH, const float* deltax,
 
 using namespace rg;
 
-namespace rg {
-int hii_reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out,
-                        cudaStream_t st);
-}
 
 extern "C" {
 
@@ -90,18 +86,12 @@ int rg_delta_T(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const 
                                                (1.0 + (double)redshift) / 10.0));
   const double t_rad = TCMB * (1. + (double)redshift);
   const int nblocks = 148 * 8;
-  if (!ctx->partials || ctx->partials_elems < (size_t)nblocks) {
-    if (ctx->partials) cudaFree(ctx->partials);
-    ctx->partials = nullptr;
-    ctx->partials_elems = 0;
-    RG_CUDA_TRY(ctx, cudaMalloc((void**)&ctx->partials, sizeof(double) * nblocks));
-    ctx->partials_elems = nblocks;
-  }
+  if (!ensure_partials(ctx, (size_t)nblocks)) return set_error(ctx, RG_ENOMEM, "partials");
   int rc = delta_T_launch(ctx, n, g->xH, g->deltax, g->TS_box, g->delta_T, const_factor, t_rad,
                           p->Flag_IncludeSpinTemp, p->Flag_IncludePecVelsFor21cm > 1, redshift, ctx->partials,
                           nblocks, st);
   if (rc) return rc;
-  if ((rc = hii_reduce_partials(ctx, ctx->partials, nblocks, 1, ctx->d_sums, st))) return rc;
+  if ((rc = reduce_partials(ctx, ctx->partials, nblocks, 1, ctx->d_sums, st))) return rc;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double), cudaMemcpyDeviceToHost, st));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   // the reference divides by N^3 before its Allreduce (BrightnessTemperature.c:528); on one rank

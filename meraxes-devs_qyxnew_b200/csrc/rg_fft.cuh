@@ -185,7 +185,15 @@ constexpr int plan_product() {
   return p;
 }
 
-// run stage s: fill v from `load(pos)`, twiddle, DFT
+// Stage-0 input position of register slot `slot` (0 <= slot < N/T) of thread t.
+template <int N>
+__device__ __forceinline__ int stage0_pos(int t, int slot) {
+  constexpr int R = Plan<N>::R[0];
+  constexpr int T = Plan<N>::T;
+  return t + (slot / R) * T + (slot % R) * (N / R);
+}
+
+// run stage s: fill v from `load(pos, slot)`, twiddle, DFT
 template <int N, int s, bool INV, class Load>
 __device__ __forceinline__ void stage_compute(cf* v, int t, const cf* __restrict__ tw, Load&& load) {
   constexpr int T = Plan<N>::T;
@@ -197,7 +205,7 @@ __device__ __forceinline__ void stage_compute(cf* v, int t, const cf* __restrict
   for (int k = 0; k < K; ++k) {
     const int j = t + k * T;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[k * R + r] = load(j + r * (N / R));
+    for (int r = 0; r < R; ++r) v[k * R + r] = load(j + r * (N / R), k * R + r);
     if constexpr (NS > 1) {
       const int jm = j % NS;
 #pragma unroll
@@ -233,7 +241,7 @@ __device__ __forceinline__ void stages_from(cf* v, int t, cf* xbuf, Addr&& addr,
     __syncthreads();  // every thread is done reading xbuf
     stage_emit<N, s>(v, t, [&](int p, cf x) { xbuf[addr(p)] = x; });
     __syncthreads();
-    stage_compute<N, s + 1, INV>(v, t, tw, [&](int p) { return xbuf[addr(p)]; });
+    stage_compute<N, s + 1, INV>(v, t, tw, [&](int p, int) { return xbuf[addr(p)]; });
     stages_from<N, s + 1, INV>(v, t, xbuf, addr, tw, store);
   } else {
     stage_emit<N, s>(v, t, store);
@@ -241,7 +249,8 @@ __device__ __forceinline__ void stages_from(cf* v, int t, cf* xbuf, Addr&& addr,
 }
 
 // Full transform of one line by thread t (0 <= t < Plan<N>::T):
-//   load(p)        -> input element at position p
+//   load(p, slot)  -> input element at position p, held in register slot `slot`
+//                     (stage0_pos<N>(t, slot) == p)
 //   addr(p)        -> index into xbuf of position p of this thread's line (exchange buffer)
 //   store(p, val)  <- output element at position p
 // Every thread of the block must call it (it contains block barriers when S > 1).

@@ -1,12 +1,22 @@
-// Excursion-set (find_HII_bubbles) step on sm_100a: the forward r2c of the source grids, and
-// per filter radius the inverse chain x (window applied on load) -> y -> z-c2r fused with the
-// aliasing clamp and the barrier test, so the per-cell state (xH, z_at_ionization, J_21,
-// temperature) is touched once per radius.  The last radius also runs the closing pass
-// (temperatures and the FP64 global sums).
+// Excursion-set step (_find_HII_bubbles, src/core/find_HII_bubbles.c:86-710) on sm_100a.
+//
+// Per snapshot: one forward r2c of each grid the barrier test reads (deltax, stars, [x_e],
+// [effective_bhm]); then the filter radii in batches of KB:
+//   x pass : each block loads its spectrum tile once and writes KB windowed, x-transformed
+//            copies (one per radius of the batch)
+//   y pass : in place over the KB x G work grids
+//   z pass : per block of rows, for each radius of the batch in order: c2r of the G grids into
+//            shared memory, then the aliasing clamp and the barrier test per cell.
+// Until the last radius the per-cell state is two bits (ionized this snapshot; z_at_ionization
+// still < 0), kept in registers within a batch and in a packed word array between batches;
+// z_at_ionization and J_21 are written only where a cell first ionizes.  The last radius also
+// computes the partial xH and runs the closing pass (temperatures and FP64 global sums).
 #include <cuda_runtime.h>
 #include <math.h>
 
 #include <cstdio>
+#include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "rg_internal.h"
@@ -35,6 +45,61 @@ __global__ void k_window_table(float* wtab, int n2max, const double* __restrict_
       w = exp(-g * g / 2.0);
     }
     wtab[(size_t)r * (n2max + 1) + n2] = (float)w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// inverse x pass with the window and a batch of radii: grid g of spec (spec + g * stride) is
+// read once per block; radius r of the batch is written to work + (r * ng + g) * stride.
+// Radius r uses window row wrows + r * wpitch, or none when r == unfiltered.
+
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<N>::BX))
+    k_hii_x(const cf* __restrict__ spec, size_t stride, int ng, cf* __restrict__ work, int nr,
+            const float* __restrict__ wrows, int wpitch, int unfiltered, const cf* __restrict__ g_tw) {
+  constexpr int T = Cfg<N>::T, B = Cfg<N>::BX, V = Cfg<N>::V;
+  extern __shared__ cf smem[];
+  cf* s_tw = smem;
+  cf* xbuf = smem + N;
+  const int kz = blockIdx.y;
+  const int b = threadIdx.x % B, t = threadIdx.x / B;
+  const int y = blockIdx.x * B + b;
+  const size_t col = (size_t)kz * N * N + y;
+  load_twiddles<N>(s_tw, g_tw);
+  // |k|^2 index of each register slot: nx from the position, ny from the column
+  int n2[V];
+  const int ny = y > N / 2 ? y - N : y;
+#pragma unroll
+  for (int sl = 0; sl < V; ++sl) {
+    const int p = stage0_pos<N>(t, sl);
+    const int nx = p > N / 2 ? p - N : p;
+    n2[sl] = nx * nx + ny * ny + kz * kz;
+  }
+  __syncthreads();
+  // Radius outer, grid inner: the window gathers (scattered 4-byte reads of the table) are
+  // shared by all grids; a grid's spectrum tile is read from HBM at the first radius and
+  // from L1/L2 after that.
+  for (int r = 0; r < nr; ++r) {
+    float wv[V];
+    if (r == unfiltered) {
+#pragma unroll
+      for (int sl = 0; sl < V; ++sl) wv[sl] = 1.f;
+    } else {
+      const float* wr = wrows + (size_t)r * wpitch;
+#pragma unroll
+      for (int sl = 0; sl < V; ++sl) wv[sl] = __ldg(wr + n2[sl]);
+    }
+    for (int g = 0; g < ng; ++g) {
+      const cf* src = spec + g * stride;
+      cf* dst = work + ((size_t)r * ng + g) * stride;
+      line_fft<N, true>(
+          t, xbuf, s_tw,
+          [&](int p, int sl) {
+            const cf v = src[col + (size_t)p * N];
+            return cf{v.x * wv[sl], v.y * wv[sl]};
+          },
+          [&](int p) { return line_addr<N, B>(p, b); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
+    }
   }
 }
 
@@ -99,123 +164,186 @@ __device__ __forceinline__ void block_sum(double (&acc)[K], double* out) {
   }
 }
 
-// Per-cell clamp and barrier test (find_HII_bubbles.c:373-544); FINAL adds the closing pass
-// (:577-645).  Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then
-// effective_bhm (BH feedback).
-template <bool FINAL>
-struct EpiHii {
-  HiiRadius r;
-  HiiConst c;
-  HiiState s;
-
-  template <int N, int ROWS, int NTH>
-  __device__ __forceinline__ void run(const float* rt, int x, int y0) const {
-    constexpr int PADW = 2 * (N / 2 + 1);
-    constexpr int RP = N + 1;
-    double acc[HII_NSUM];
-#pragma unroll
-    for (int i = 0; i < HII_NSUM; ++i) acc[i] = 0.0;
-    const int gx = c.spin ? 2 : -1;
-    const int gb = c.bh ? (c.spin ? 3 : 2) : -1;
-    // Cells are taken CH at a time: the global reads of a chunk are issued together before
-    // any of its stores, so their latencies overlap (the state pointers may alias as far as
-    // the compiler knows, which would otherwise serialise load -> store -> load).
-    constexpr int NCELL = ROWS * N;
-    constexpr int CH = 8;
-    static_assert(NCELL % NTH == 0, "block covers whole rows");
-    constexpr int IT = NCELL / NTH;
-    constexpr int CHK = IT < CH ? IT : CH;
-    static_assert(IT % CHK == 0, "chunking");
-    for (int it0 = 0; it0 < IT; it0 += CHK) {
-      float xh_in[CHK], zin_in[CHK];
-#pragma unroll
-      for (int u = 0; u < CHK; ++u) {
-        const int i = threadIdx.x + (it0 + u) * NTH;
-        const int z = i % N, row = i / N;
-        const size_t ir = ((size_t)x * N + y0 + row) * N + z;
-        xh_in[u] = r.first ? 1.f : __ldg(s.xH + ir);
-        zin_in[u] = __ldg(s.z_in + ir);
-      }
-#pragma unroll
-      for (int u = 0; u < CHK; ++u) {
-      const int i = threadIdx.x + (it0 + u) * NTH;
-      const int z = i % N, row = i / N;
-      const int y = y0 + row;
-      const size_t ir = ((size_t)x * N + y) * N + z;
-      const size_t ip = ((size_t)x * N + y) * PADW + z;
-      const float dx = fmaxf(rt[row * RP + z], -1.f + REL_TOL);
-      float st = fmaxf(rt[(ROWS + row) * RP + z], 0.f);
-      if (st < ABS_TOL) st = 0.f;
-      float xe = 0.f, bhm = 0.f;
-      if (gx >= 0) {
-        xe = fmaxf(rt[(gx * ROWS + row) * RP + z], 0.f);
-        if (xe < ABS_TOL) xe = 0.f;
-        xe = fminf(xe, 0.999f);
-      }
-      if (gb >= 0) {
-        bhm = fmaxf(rt[(gb * ROWS + row) * RP + z], 0.f);
-        if (bhm < ABS_TOL) bhm = 0.f;
-      }
-      const double dom = 1.0 + (double)dx;
-      const double fcs = (double)st / dom;
-      const double fbh = c.bh ? (double)bhm / dom : 0.0;
-      const double nf = c.spin ? 1.0 - (double)xe : 1.0;
-      const double lhs = (fbh + fcs) * r.fcoll_pref;
-      float xH = xh_in[u];
-      float zin = zin_in[u];
-      if (lhs > nf * (1.0 + 0.0)) {
-        xH = 0.f;
-      } else if (r.last && xH > REL_TOL) {
-        float thi;
-        if (c.spin) {
-          thi = s.Tk_box[ir];
-        } else {
-          const float du = s.deltax_unf[ip];
-          thi = (float)((double)c.TK * (1.0 + (double)(c.cT_ad * du)));
-        }
-        s.temp[ir] = partial_T(thi, xH);
-        float v = (float)(nf - lhs);
-        v = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
-        xH = v;
-      }
-      if (xH < REL_TOL && zin < 0.f) {
-        zin = c.redshift;
-        s.z_in[ir] = zin;
-        if (c.uvb == 1) {
-          float j = st * r.J_aux;
-          if (c.bh) j += bhm * r.J_aux_bh;
-          s.J21[ir] = j;
-        }
-      }
-      s.xH[ir] = xH;
-      if (FINAL) {
-        const float du = s.deltax_unf[ip];
-        const double domu = 1.0 + (double)du;
-        float temp = s.temp[ir];
-        if (zin > 0.f && xH < REL_TOL) temp = fully_ionized_T(zin, c.redshift, du);
-        if (c.spin) {
-          const float tk = s.Tk_box[ir];
-          if (temp < tk) temp = tk;
-        } else {
-          const float thistk = (float)((double)c.TK * (1.0 + (double)(c.cT_ad * du)));
-          if (temp < thistk) temp = thistk;
-        }
-        s.temp[ir] = temp;
-        acc[0] += (double)xH;
-        // acc[1] and acc[6]: r_bubble is written only on the recombination branch
-        // (find_HII_bubbles.c:490-508), which this library rejects, so it stays 0.
-        acc[2] += (double)s.wsfr[ip];
-        if (s.bhar != nullptr) acc[3] += (double)s.bhar[ip];
-        acc[4] += (double)temp;
-        acc[5] += (double)xH * domu;
-        acc[7] += (double)temp * domu;
-        acc[8] += domu;
-      }
-      }
-    }
-    if (FINAL) block_sum<NTH, HII_NSUM>(acc, s.partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * HII_NSUM);
-  }
+struct HiiBatch {
+  int nr;             // radii in this batch
+  int first;          // the batch starts the snapshot (state comes from z_at_ionization)
+  double fcoll_pref[KB_MAX];
+  float J_aux[KB_MAX], J_aux_bh[KB_MAX];
 };
+
+struct HiiState {
+  float* xH;
+  float* z_in;
+  float* J21;
+  float* temp;
+  const float* Tk_box;
+  const float* deltax_unf;   // padded
+  const float* wsfr;         // padded
+  const float* bhar;         // padded, may be null
+  uint32_t* bits;            // [2][nblocks][W][NTH]
+  double* partials;          // [nblocks][HII_NSUM]
+};
+
+// z pass of a batch.  FINAL: the batch ends with the snapshot's last (unfiltered) radius.
+// Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then effective_bhm (BH).
+template <int N, int NG, bool FINAL>
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<N>::QZ))
+    k_hii_z(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
+            HiiState s) {
+  constexpr int T = Cfg<N>::T, Q = Cfg<N>::QZ, NTH = T * Q, ROWS = 2 * Q, RP = Cfg<N>::RT_PITCH;
+  constexpr int PADW = 2 * (N / 2 + 1);
+  constexpr int IT = ROWS * N / NTH;   // cells per thread
+  constexpr int W = (IT + 31) / 32;    // bit words per thread
+  static_assert(ROWS * N % NTH == 0, "whole rows per block");
+  extern __shared__ cf smem[];
+  cf* s_tw = smem;
+  cf* xbuf = smem + N;
+  float* rt = reinterpret_cast<float*>(xbuf + line_buf<N, Q>());
+  const int x = blockIdx.y, y0 = blockIdx.x * ROWS;
+  const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+  const size_t nwords = (size_t)gridDim.x * gridDim.y * W * NTH;
+  load_twiddles<N>(s_tw, g_tw);
+
+  // per-cell state bits: A = z_at_ionization still < 0, I = ionized at a radius of this snapshot.
+  // Cell it of this thread is block cell threadIdx.x + it * NTH, bit it % 32 of word it / 32.
+  uint32_t A[W], I[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    if (bt.first) {
+      uint32_t a = 0u;
+      const int nb = IT - 32 * w < 32 ? IT - 32 * w : 32;
+#pragma unroll 8
+      for (int bb = 0; bb < nb; ++bb) {
+        const int i = threadIdx.x + (32 * w + bb) * NTH;
+        const size_t ir = ((size_t)x * N + y0 + i / N) * N + i % N;
+        if (s.z_in[ir] < 0.f) a |= 1u << bb;
+      }
+      A[w] = a;
+      I[w] = 0u;
+    } else {
+      A[w] = s.bits[(blk * W + w) * NTH + threadIdx.x];
+      I[w] = s.bits[nwords + (blk * W + w) * NTH + threadIdx.x];
+    }
+  }
+  const int gx = c.spin ? 2 : -1;
+  const int gb = c.bh ? (c.spin ? 3 : 2) : -1;
+  double acc[FINAL ? HII_NSUM : 1];
+#pragma unroll
+  for (int k = 0; k < (FINAL ? HII_NSUM : 1); ++k) acc[k] = 0.0;
+
+  for (int r = 0; r < bt.nr; ++r) {
+    __syncthreads();  // rt of the previous radius is consumed
+    zfront<N, NG>(work + (size_t)r * NG * stride, stride, s_tw, xbuf, rt, x, y0);
+    const bool last = FINAL && r == bt.nr - 1;
+    const double pref = bt.fcoll_pref[r];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      uint32_t a = A[w], iw = I[w];
+      const int nb = IT - 32 * w < 32 ? IT - 32 * w : 32;
+#pragma unroll 4
+      for (int bb = 0; bb < nb; ++bb) {
+        const int i = threadIdx.x + (32 * w + bb) * NTH;
+        const int z = i % N, row = i / N;
+        const uint32_t bit = 1u << bb;
+        const float dx = fmaxf(rt[row * RP + z], -1.f + REL_TOL);
+        float st = fmaxf(rt[(ROWS + row) * RP + z], 0.f);
+        if (st < ABS_TOL) st = 0.f;
+        float xe = 0.f, bhm = 0.f;
+        if (gx >= 0) {
+          xe = fmaxf(rt[(gx * ROWS + row) * RP + z], 0.f);
+          if (xe < ABS_TOL) xe = 0.f;
+          xe = fminf(xe, 0.999f);
+        }
+        if (gb >= 0) {
+          bhm = fmaxf(rt[(gb * ROWS + row) * RP + z], 0.f);
+          if (bhm < ABS_TOL) bhm = 0.f;
+        }
+        const double dom = 1.0 + (double)dx;  // >= 1e-5 after the clamp
+        const double nf = c.spin ? 1.0 - (double)xe : 1.0;
+        // (f_bh + f_stars) * prefactor > nf with f = grid / dom, tested without the division:
+        // the two forms differ only within a few FP64 ulps of the barrier
+        const double num = c.bh ? (double)bhm + (double)st : (double)st;
+        const bool ion = num * pref > nf * (1.0 + 0.0) * dom;
+        float xH = (iw & bit) ? 0.f : 1.f;   // so far: 0 once ionized at a radius, else 1
+        const size_t cellrow = (size_t)x * N + y0 + row;
+        const size_t ir = cellrow * N + z;
+        float temp_new = -1.f;               // >= 0: partial temperature written this radius
+        if (ion) {
+          xH = 0.f;
+          iw |= bit;
+        } else if (last && xH > REL_TOL) {
+          // partially ionized: temperature of the neutral gas, xH = nf - f_coll prefactor
+          float thi;
+          if (c.spin) {
+            thi = s.Tk_box[ir];
+          } else {
+            const float du = s.deltax_unf[cellrow * PADW + z];
+            thi = (float)((double)c.TK * (1.0 + (double)(c.cT_ad * du)));
+          }
+          temp_new = partial_T(thi, xH);
+          const double fcs = (double)st / dom;
+          const double fbh = c.bh ? (double)bhm / dom : 0.0;
+          const double lhs = (fbh + fcs) * pref;
+          const float v = (float)(nf - lhs);
+          xH = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+        }
+        float zin_new = -1.f;                // > -1: set this radius
+        if (xH < REL_TOL && (a & bit)) {
+          // new ionization (find_HII_bubbles.c:531-543)
+          a &= ~bit;
+          zin_new = c.redshift;
+          s.z_in[ir] = zin_new;
+          if (c.uvb == 1) {
+            float j = st * bt.J_aux[r];
+            if (c.bh) j += bhm * bt.J_aux_bh[r];
+            s.J21[ir] = j;
+          }
+        }
+        if (FINAL && last) {
+          // closing pass (find_HII_bubbles.c:577-645)
+          const size_t ip = cellrow * PADW + z;
+          s.xH[ir] = xH;
+          const float du = s.deltax_unf[ip];
+          const double domu = 1.0 + (double)du;
+          float temp = temp_new >= 0.f ? temp_new : s.temp[ir];
+          if (xH < REL_TOL) {
+            const float zin = zin_new > -1.f ? zin_new : s.z_in[ir];
+            if (zin > 0.f) temp = fully_ionized_T(zin, c.redshift, du);
+          }
+          if (c.spin) {
+            const float tk = s.Tk_box[ir];
+            if (temp < tk) temp = tk;
+          } else {
+            const float thistk = (float)((double)c.TK * (1.0 + (double)(c.cT_ad * du)));
+            if (temp < thistk) temp = thistk;
+          }
+          s.temp[ir] = temp;
+          acc[0] += (double)xH;
+          // acc[1] and acc[6]: r_bubble is written only on the recombination branch
+          // (find_HII_bubbles.c:490-508), which this library rejects, so it stays 0.
+          acc[2] += (double)s.wsfr[ip];
+          if (s.bhar != nullptr) acc[3] += (double)s.bhar[ip];
+          acc[4] += (double)temp;
+          acc[5] += (double)xH * domu;
+          acc[7] += (double)temp * domu;
+          acc[8] += domu;
+        }
+      }
+      A[w] = a;
+      I[w] = iw;
+    }
+  }
+
+  if constexpr (!FINAL) {
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      s.bits[(blk * W + w) * NTH + threadIdx.x] = A[w];
+      s.bits[nwords + (blk * W + w) * NTH + threadIdx.x] = I[w];
+    }
+  } else {
+    block_sum<NTH, HII_NSUM>(acc, s.partials + blk * HII_NSUM);
+  }
+}
 
 // deterministic second stage: one block sums the per-block partials in a fixed order
 __global__ void k_reduce_partials(const double* __restrict__ partials, int nblocks, int nsum, double* out) {
@@ -235,7 +363,7 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nbloc
 }
 
 // ---------------------------------------------------------------------------
-// host-side launchers
+// launchers
 
 template <typename K>
 static cudaError_t prep(K kernel, size_t smem) {
@@ -243,114 +371,81 @@ static cudaError_t prep(K kernel, size_t smem) {
 }
 
 template <int N>
-size_t smem_x() { return sizeof(cf) * (N + (size_t)N * Cfg<N>::BX); }
+constexpr size_t smem_x() { return sizeof(cf) * (N + (size_t)line_buf<N, Cfg<N>::BX>()); }
 template <int N>
-size_t smem_y() { return sizeof(cf) * (N + (size_t)Cfg<N>::BY * Cfg<N>::PITCH_Y); }
+constexpr size_t smem_y() { return sizeof(cf) * (N + (size_t)Cfg<N>::BY * Cfg<N>::PITCH_P); }
 template <int N>
-size_t smem_fz() { return sizeof(cf) * (N + 2 * (size_t)Cfg<N>::QF * Cfg<N>::PITCH_F); }
-template <int N>
-size_t smem_iz(int ng) {
-  return sizeof(cf) * (N + (size_t)N * Cfg<N>::QZ) + sizeof(float) * (size_t)ng * 2 * Cfg<N>::QZ * (N + 1);
-}
+constexpr size_t smem_fz() { return sizeof(cf) * (N + 2 * (size_t)Cfg<N>::QF * Cfg<N>::PITCH_P); }
 
 template <int N>
-int launch_forward(rg_context* ctx, const float* const* d_real, cf* const* d_spec, int ng, double scale,
+int launch_forward(rg_context* ctx, const float* const* d_real, int ng, cf* spec, size_t stride, double scale,
                    cudaStream_t st) {
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
   GridPtrs src{};
-  GridPtrsW dst{};
-  GridPtrs dsrc{};
-  for (int g = 0; g < ng; ++g) {
-    src.p[g] = d_real[g];
-    dst.p[g] = d_spec[g];
-    dsrc.p[g] = d_spec[g];
-  }
+  for (int g = 0; g < ng; ++g) src.p[g] = d_real[g];
   const double nzc = (double)C::NZ * N * N;
-  {
-    const size_t sm = smem_fz<N>();
-    RG_CUDA_TRY(ctx, prep(k_fwd_z<N>, sm));
-    prof_begin(ctx, "fwd_z_r2c", st);
-    k_fwd_z<N><<<dim3(N / (2 * C::QF), N, ng), C::T * C::QF, sm, st>>>(src, dst, tw);
-    prof_end(ctx, ng * (4.0 * N * N * N + 8.0 * nzc), st);
-    RG_CUDA_TRY(ctx, cudaGetLastError());
-  }
-  {
-    const size_t sm = smem_y<N>();
-    RG_CUDA_TRY(ctx, prep(k_pass_y<N, false>, sm));
-    prof_begin(ctx, "fwd_y_c2c", st);
-    k_pass_y<N, false><<<dim3(N / C::BY, C::NZ, ng), C::T * C::BY, sm, st>>>(dst, tw);
-    prof_end(ctx, ng * 16.0 * nzc, st);
-    RG_CUDA_TRY(ctx, cudaGetLastError());
-  }
-  {
-    const size_t sm = smem_x<N>();
-    RG_CUDA_TRY(ctx, prep(k_pass_x<N, false, LoadPlain>, sm));
-    prof_begin(ctx, "fwd_x_c2c", st);
-    k_pass_x<N, false, LoadPlain><<<dim3(N / C::BX, C::NZ, ng), C::T * C::BX, sm, st>>>(LoadPlain{dsrc}, dst, tw,
-                                                                                          (float)scale);
-    prof_end(ctx, ng * 16.0 * nzc, st);
-    RG_CUDA_TRY(ctx, cudaGetLastError());
-  }
+  RG_CUDA_TRY(ctx, prep(k_fwd_z<N>, smem_fz<N>()));
+  prof_begin(ctx, "fwd_z_r2c", st);
+  k_fwd_z<N><<<dim3(N / (2 * C::QF), N, ng), C::T * C::QF, smem_fz<N>(), st>>>(src, spec, stride, tw);
+  prof_end(ctx, ng * (4.0 * N * N * N + 8.0 * nzc), st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  RG_CUDA_TRY(ctx, prep(k_pass_y<N, false>, smem_y<N>()));
+  prof_begin(ctx, "fwd_y_c2c", st);
+  k_pass_y<N, false><<<dim3(N / C::BY, C::NZ, ng), C::T * C::BY, smem_y<N>(), st>>>(spec, stride, tw);
+  prof_end(ctx, ng * 16.0 * nzc, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  RG_CUDA_TRY(ctx, prep(k_pass_x_fwd<N>, smem_x<N>()));
+  prof_begin(ctx, "fwd_x_c2c", st);
+  k_pass_x_fwd<N><<<dim3(N / C::BX, C::NZ, ng), C::T * C::BX, smem_x<N>(), st>>>(spec, stride, tw, (float)scale);
+  prof_end(ctx, ng * 16.0 * nzc, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 
+// inverse x (window, batch of nr radii) and y passes
 template <int N>
-int launch_inverse_xy(rg_context* ctx, cf* const* d_spec, cf* const* d_work, int ng, const float* wrow,
-                      cudaStream_t st) {
+int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, cf* work, size_t stride, int nr, const float* wrows,
+                      int wpitch, int unfiltered, cudaStream_t st) {
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
-  GridPtrs src{};
-  GridPtrsW dst{};
-  for (int g = 0; g < ng; ++g) {
-    src.p[g] = d_spec[g];
-    dst.p[g] = d_work[g];
-  }
   const double nzc = (double)C::NZ * N * N;
-  {
-    const size_t sm = smem_x<N>();
-    RG_CUDA_TRY(ctx, prep(k_pass_x<N, true, LoadWindow<N>>, sm));
-    prof_begin(ctx, "inv_x_c2c_window", st);
-    k_pass_x<N, true, LoadWindow<N>><<<dim3(N / C::BX, C::NZ, ng), C::T * C::BX, sm, st>>>(
-        LoadWindow<N>{src, wrow}, dst, tw, 1.f);
-    prof_end(ctx, ng * 16.0 * nzc, st);
-    RG_CUDA_TRY(ctx, cudaGetLastError());
-  }
-  {
-    const size_t sm = smem_y<N>();
-    RG_CUDA_TRY(ctx, prep(k_pass_y<N, true>, sm));
-    prof_begin(ctx, "inv_y_c2c", st);
-    k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, ng), C::T * C::BY, sm, st>>>(dst, tw);
-    prof_end(ctx, ng * 16.0 * nzc, st);
-    RG_CUDA_TRY(ctx, cudaGetLastError());
-  }
+  RG_CUDA_TRY(ctx, prep(k_hii_x<N>, smem_x<N>()));
+  prof_begin(ctx, "inv_x_c2c_window", st);
+  k_hii_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smem_x<N>(), st>>>(spec, stride, ng, work, nr, wrows, wpitch,
+                                                                        unfiltered, tw);
+  prof_end(ctx, ng * 8.0 * nzc * (1 + nr), st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  RG_CUDA_TRY(ctx, prep(k_pass_y<N, true>, smem_y<N>()));
+  prof_begin(ctx, "inv_y_c2c", st);
+  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, ng * nr), C::T * C::BY, smem_y<N>(), st>>>(work, stride, tw);
+  prof_end(ctx, ng * nr * 16.0 * nzc, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 
 template <int N, int NG, bool FINAL>
-int launch_inv_z_test3(rg_context* ctx, cf* const* d_work, const HiiRadius& r, const HiiConst& c, const HiiState& s,
-                       cudaStream_t st, int* nblocks) {
+int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch& bt, const HiiConst& c,
+                  const HiiState& s, cudaStream_t st, int* nblocks) {
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
-  GridPtrs w{};
-  for (int g = 0; g < NG; ++g) w.p[g] = d_work[g];
-  const size_t sm = smem_iz<N>(NG);
-  RG_CUDA_TRY(ctx, prep(k_inv_z<N, NG, EpiHii<FINAL>>, sm));
+  const size_t sm = zfront_smem_bytes<N>(NG);
+  RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL>, sm));
   const dim3 grid(N / (2 * C::QZ), N);
-  // algorithmic bytes: the Hermitian halves read once, xH read (after the first radius)
-  // and written, z_at_ionization read; the closing pass adds deltax, weighted_sfr,
-  // effective_bhar, Tk_box reads and the temperature read + write.
+  // algorithmic bytes: the Hermitian halves of NG grids per radius, z_at_ionization on the
+  // first batch; the closing pass writes xH and temperature and reads deltax, weighted_sfr,
+  // [effective_bhar], [Tk_box]
   const double n3 = (double)N * N * N, nzc = (double)C::NZ * N * N;
-  double bytes = NG * 8.0 * nzc + (r.first ? 0.0 : 4.0 * n3) + 4.0 * n3 + 4.0 * n3;
-  if (FINAL) bytes += 4.0 * n3 * (2 + (s.bhar != nullptr) + (s.Tk_box != nullptr) + 2);
+  double bytes = bt.nr * NG * 8.0 * nzc + (bt.first ? 4.0 * n3 : 0.0);
+  if (FINAL) bytes += 4.0 * n3 * (2 + 2 + (s.bhar != nullptr) + (s.Tk_box != nullptr));
   prof_begin(ctx, FINAL ? "inv_z_c2r_test_final" : "inv_z_c2r_test", st);
-  k_inv_z<N, NG, EpiHii<FINAL>><<<grid, C::T * C::QZ, sm, st>>>(w, tw, EpiHii<FINAL>{r, c, s});
+  k_hii_z<N, NG, FINAL><<<grid, C::T * C::QZ, sm, st>>>(work, stride, tw, bt, c, s);
   prof_end(ctx, bytes, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   if (nblocks) *nblocks = (int)(grid.x * grid.y);
@@ -358,33 +453,37 @@ int launch_inv_z_test3(rg_context* ctx, cf* const* d_work, const HiiRadius& r, c
 }
 
 template <int N>
-int launch_inv_z_test(rg_context* ctx, cf* const* d_work, int ngrids, const HiiRadius& r, const HiiConst& c,
-                      const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
-  if (ngrids == 2)
-    return fin ? launch_inv_z_test3<N, 2, true>(ctx, d_work, r, c, s, st, nblocks)
-               : launch_inv_z_test3<N, 2, false>(ctx, d_work, r, c, s, st, nblocks);
-  if (ngrids == 3)
-    return fin ? launch_inv_z_test3<N, 3, true>(ctx, d_work, r, c, s, st, nblocks)
-               : launch_inv_z_test3<N, 3, false>(ctx, d_work, r, c, s, st, nblocks);
-  return fin ? launch_inv_z_test3<N, 4, true>(ctx, d_work, r, c, s, st, nblocks)
-             : launch_inv_z_test3<N, 4, false>(ctx, d_work, r, c, s, st, nblocks);
+int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
+                 const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
+  if (ng == 2)
+    return fin ? launch_hii_z3<N, 2, true>(ctx, work, stride, bt, c, s, st, nblocks)
+               : launch_hii_z3<N, 2, false>(ctx, work, stride, bt, c, s, st, nblocks);
+  if (ng == 3)
+    return fin ? launch_hii_z3<N, 3, true>(ctx, work, stride, bt, c, s, st, nblocks)
+               : launch_hii_z3<N, 3, false>(ctx, work, stride, bt, c, s, st, nblocks);
+  return fin ? launch_hii_z3<N, 4, true>(ctx, work, stride, bt, c, s, st, nblocks)
+             : launch_hii_z3<N, 4, false>(ctx, work, stride, bt, c, s, st, nblocks);
+}
+
+// words of packed state per bit kind
+template <int N>
+size_t hii_bit_words() {
+  using C = Cfg<N>;
+  constexpr int NTH = C::T * C::QZ, IT = 2 * C::QZ * N / NTH, W = (IT + 31) / 32;
+  return (size_t)(N / (2 * C::QZ)) * N * W * NTH;
 }
 
 template <int N>
-int launch_debug_inverse(rg_context* ctx, cf* spec, cf* work, const float* wrow, float* out, cudaStream_t st) {
-  cf* sp[1] = {spec};
-  cf* wk[1] = {work};
-  int rc = launch_inverse_xy<N>(ctx, sp, wk, 1, wrow, st);
+int launch_debug_inverse(rg_context* ctx, const cf* spec, cf* work, const float* wrow, float* out, cudaStream_t st) {
+  const size_t stride = (size_t)Cfg<N>::NZ * N * N;
+  int rc = launch_inverse_xy<N>(ctx, spec, 1, work, stride, 1, wrow, 0, wrow ? -1 : 0, st);
   if (rc) return rc;
   const cf* tw;
-  rc = twiddles_for(ctx, N, &tw);
-  if (rc) return rc;
+  if ((rc = twiddles_for(ctx, N, &tw))) return rc;
   using C = Cfg<N>;
-  GridPtrs w{};
-  w.p[0] = work;
-  const size_t sm = smem_iz<N>(1);
-  RG_CUDA_TRY(ctx, prep(k_inv_z<N, 1, EpiPadded>, sm));
-  k_inv_z<N, 1, EpiPadded><<<dim3(N / (2 * C::QZ), N), C::T * C::QZ, sm, st>>>(w, tw, EpiPadded{out});
+  const size_t sm = zfront_smem_bytes<N>(1);
+  RG_CUDA_TRY(ctx, prep(k_inv_z_padded<N>, sm));
+  k_inv_z_padded<N><<<dim3(N / (2 * C::QZ), N), C::T * C::QZ, sm, st>>>(work, tw, out);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
@@ -406,32 +505,43 @@ int launch_debug_inverse(rg_context* ctx, cf* spec, cf* work, const float* wrow,
     default: return set_error(ctx, RG_EUNSUPPORTED, "ReionGridDim not in {8,16,24,32,48,64,96,128,192,256,384,512}"); \
   }
 
-int hii_forward(rg_context* ctx, int n, const float* const* d_real, cf* const* d_spec, int ng, double scale,
+#define RG_DISPATCH_N_VAL(n, call, dflt)       \
+  switch (n) {                                 \
+    case 8: { constexpr int NN = 8; return call; } \
+    case 16: { constexpr int NN = 16; return call; } \
+    case 24: { constexpr int NN = 24; return call; } \
+    case 32: { constexpr int NN = 32; return call; } \
+    case 48: { constexpr int NN = 48; return call; } \
+    case 64: { constexpr int NN = 64; return call; } \
+    case 96: { constexpr int NN = 96; return call; } \
+    case 128: { constexpr int NN = 128; return call; } \
+    case 192: { constexpr int NN = 192; return call; } \
+    case 256: { constexpr int NN = 256; return call; } \
+    case 384: { constexpr int NN = 384; return call; } \
+    case 512: { constexpr int NN = 512; return call; } \
+    default: return dflt;                      \
+  }
+
+int fft_forward(rg_context* ctx, int n, const float* const* d_real, int ng, cf* spec, size_t stride, double scale,
                 cudaStream_t st) {
   if (ng > MAXG) return set_error(ctx, RG_EINVAL, "too many grids in one forward launch");
-  RG_DISPATCH_N(n, launch_forward<NN>(ctx, d_real, d_spec, ng, scale, st));
+  RG_DISPATCH_N(n, launch_forward<NN>(ctx, d_real, ng, spec, stride, scale, st));
 }
 
-int hii_inverse_xy(rg_context* ctx, int n, cf* const* d_spec, cf* const* d_work, int ng, const float* wrow,
-                   cudaStream_t st) {
-  if (ng > MAXG) return set_error(ctx, RG_EINVAL, "too many grids in one inverse launch");
-  RG_DISPATCH_N(n, launch_inverse_xy<NN>(ctx, d_spec, d_work, ng, wrow, st));
+static int inverse_xy(rg_context* ctx, int n, const cf* spec, int ng, cf* work, size_t stride, int nr,
+                      const float* wrows, int wpitch, int unfiltered, cudaStream_t st) {
+  RG_DISPATCH_N(n, launch_inverse_xy<NN>(ctx, spec, ng, work, stride, nr, wrows, wpitch, unfiltered, st));
 }
 
-int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int ngrids, const HiiRadius& r, const HiiConst& c,
-                       const HiiState& s, bool final_pass, cudaStream_t st, int* nblocks_out) {
-  if (ngrids < 2 || ngrids > 4) return set_error(ctx, RG_EINVAL, "the barrier test reads 2 to 4 grids");
-  RG_DISPATCH_N(n, launch_inv_z_test<NN>(ctx, d_work, ngrids, r, c, s, final_pass, st, nblocks_out));
+static int hii_z(rg_context* ctx, int n, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
+                 const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
+  RG_DISPATCH_N(n, launch_hii_z<NN>(ctx, work, stride, ng, bt, c, s, fin, st, nblocks));
 }
 
-int debug_inverse_to_padded(rg_context* ctx, int n, cf* d_spec, cf* d_work, const float* wrow, float* d_out,
-                            cudaStream_t st) {
-  RG_DISPATCH_N(n, launch_debug_inverse<NN>(ctx, d_spec, d_work, wrow, d_out, st));
-}
+static size_t bit_words(int n) { RG_DISPATCH_N_VAL(n, hii_bit_words<NN>(), (size_t)0); }
 
-int hii_window_table(rg_context* ctx, int n, double box, const double* d_radii, int nr, int ftype, float* d_wtab,
-                     int n2max, cudaStream_t st) {
-  (void)n;
+int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int ftype, float* d_wtab, int n2max,
+                 cudaStream_t st) {
   const double delta_k = 2.0 * M_PI / box;
   const int bx = (n2max + 1 + 255) / 256;
   k_window_table<<<dim3(bx < 1024 ? bx : 1024, nr), 256, 0, st>>>(d_wtab, n2max, d_radii, nr, delta_k, ftype);
@@ -439,11 +549,166 @@ int hii_window_table(rg_context* ctx, int n, double box, const double* d_radii, 
   return RG_OK;
 }
 
-int hii_reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out,
-                        cudaStream_t st) {
+int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out, cudaStream_t st) {
   k_reduce_partials<<<1, 256, 0, st>>>(partials, nblocks, nsum, d_out);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
+}
+
+template <typename T>
+static int ensure_buf(rg_context* ctx, T** ptr, size_t* have, size_t need) {
+  if (*ptr && *have >= need) return RG_OK;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *have = 0;
+  cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * need);
+  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  *have = need;
+  return RG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the snapshot
+
+int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out) {
+  int rc;
+  cudaStream_t st = ctx->stream;
+  const int N = ctx->N;
+  const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
+  const double redshift = s->ZZ[s->snapshot];
+  const double box_size = p->BoxSize;
+  const double pixel_volume = std::pow(box_size / (double)N, 3);
+  const Units u = make_units(p);
+  const double sfr_timescale = p->ReionSfrTimescale * hubble_time_at(p, redshift);
+  const double tk_d = T_RECFAST(ctx->tables, (float)redshift);
+  if (tk_d < 0) return set_error(ctx, RG_ETABLE, "T_RECFAST called beyond its table");
+  HiiConst c;
+  c.redshift = (float)redshift;
+  c.TK = (float)tk_d;
+  c.cT_ad = cT_approx((float)redshift);
+  c.uvb = p->ReionUVBFlag;
+  c.spin = spin;
+  c.bh = bh;
+
+  // Grids to transform: the ones the barrier test reads, in its order.  weighted_sfr (and
+  // effective_bhar) feed only Gamma12 on the recombination branch, so their filtered fields
+  // are never read here; the plain mode transforms weighted_sfr anyway, as the reference does.
+  const float* srcs[5];
+  int ng = 0;
+  srcs[ng++] = g->deltax;
+  srcs[ng++] = g->stars;
+  if (spin) srcs[ng++] = g->x_e_box;
+  if (bh) srcs[ng++] = g->effective_bhm;
+  const int ntest = ng;
+  const bool plain = ctx->mode == RG_MODE_PLAIN;
+  if (plain) srcs[ng++] = g->weighted_sfr;
+
+  const size_t nc = (size_t)(N / 2 + 1) * N * N;
+  auto sched = radius_schedule(p, redshift);
+  const int nr = (int)sched.size();
+  int kb = plain ? 1 : (ctx->radius_batch > 0 ? ctx->radius_batch : 8);
+  if (kb > KB_MAX) kb = KB_MAX;
+  if (kb > nr) kb = nr;
+  if ((rc = ensure_buf(ctx, &ctx->spec, &ctx->spec_elems, nc * ng))) return rc;
+  if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc * ng * kb))) return rc;
+  const size_t nw = bit_words(N);
+  if ((rc = ensure_buf(ctx, &ctx->bits, &ctx->bits_elems, 2 * nw))) return rc;
+  if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
+
+  // window table for all radii
+  const int n2max = 3 * (N / 2) * (N / 2);
+  std::vector<double> radii(nr);
+  for (int i = 0; i < nr; ++i) radii[i] = sched[i].first;
+  if ((rc = ensure_buf(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
+  if ((rc = ensure_buf(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
+  if ((rc = window_table(ctx, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st))) return rc;
+
+  // r_bubble is only written on the recombination branch: zero it once
+  RG_CUDA_TRY(ctx, cudaMemsetAsync(g->r_bubble, 0, sizeof(float) * (size_t)N * N * N, st));
+  double* partials = ensure_partials(ctx, (size_t)N * N * HII_NSUM);
+  if (!partials) return set_error(ctx, RG_ENOMEM, "partials");
+
+  HiiState hs;
+  hs.xH = g->xH;
+  hs.z_in = g->z_at_ionization;
+  hs.J21 = g->J_21_at_ionization;
+  hs.temp = g->temp_kinetic_all_gas;
+  hs.Tk_box = spin ? g->Tk_box : nullptr;
+  hs.deltax_unf = g->deltax;
+  hs.wsfr = g->weighted_sfr;
+  hs.bhar = bh ? g->effective_bhar : nullptr;
+  hs.bits = ctx->bits;
+  hs.partials = partials;
+
+  int nblocks = 0;
+  for (int r0 = 0; r0 < nr; r0 += kb) {
+    const int cnt = std::min(kb, nr - r0);
+    const bool fin = (r0 + cnt == nr);
+    HiiBatch bt;
+    std::memset(&bt, 0, sizeof(bt));
+    bt.nr = cnt;
+    bt.first = (r0 == 0);
+    for (int k = 0; k < cnt; ++k) {
+      const double R = sched[r0 + k].first;
+      const double M_mean = rtom(p, R);
+      // find_HII_bubbles.c:430-442
+      double Gamma_R_prefactor = (1.0 + redshift) * (1.0 + redshift) * R * p->UnitLength_in_cm / pixel_volume *
+                                 std::pow(p->UnitLength_in_cm, -3.);
+      Gamma_R_prefactor *= (p->UnitMass_in_g / u.UnitTime_in_s) / PROTONMASS * p->ReionNionPhotPerBary;
+      bt.J_aux[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
+                            p->ReionAlphaUV);
+      bt.J_aux_bh[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias /
+                               sfr_timescale * p->ReionAlphaUVBH);
+      bt.fcoll_pref[k] = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R * R * R;
+    }
+    // the snapshot's last radius is unfiltered (find_HII_bubbles.c:313)
+    const int unf = fin ? cnt - 1 : -1;
+    if ((rc = inverse_xy(ctx, N, ctx->spec, ng, ctx->work, nc, cnt, ctx->wtab + (size_t)r0 * (n2max + 1), n2max + 1,
+                         unf, st)))
+      return rc;
+    if ((rc = hii_z(ctx, N, ctx->work, nc, ntest, bt, c, hs, fin, st, &nblocks))) return rc;
+  }
+  if ((rc = reduce_partials(ctx, partials, nblocks, HII_NSUM, ctx->d_sums, st))) return rc;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * HII_NSUM, cudaMemcpyDeviceToHost, st));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  prof_resolve(ctx);
+
+  const double n3 = std::pow((double)N, 3);
+  const double* S = ctx->h_sums;
+  const double mass_weight = S[8];
+  out->volume_weighted_global_xH = S[0] / n3;
+  out->volume_weighted_global_r_bubble = S[1] / n3;
+  out->volume_weighted_global_weighted_sfr = S[2] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
+  out->volume_weighted_global_effective_bhar =
+      S[3] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
+  out->volume_weighted_global_temp_kinetic_all_gas = S[4] / n3;
+  out->mass_weighted_global_xH = S[5] / mass_weight;
+  out->mass_weighted_global_r_bubble = S[6] / mass_weight;
+  out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
+  out->n_radii = nr;
+  return RG_OK;
+}
+
+int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype) {
+  int rc;
+  cudaStream_t st = ctx->stream;
+  const int N = ctx->N;
+  const size_t nc = (size_t)(N / 2 + 1) * N * N;
+  if ((rc = ensure_buf(ctx, &ctx->spec, &ctx->spec_elems, nc))) return rc;
+  if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc))) return rc;
+  const float* srcs[1] = {d_in};
+  if ((rc = fft_forward(ctx, N, srcs, 1, ctx->spec, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
+  const float* wrow = nullptr;
+  if (ftype >= 0) {
+    const int n2max = 3 * (N / 2) * (N / 2);
+    if ((rc = ensure_buf(ctx, &ctx->d_radii, &ctx->d_radii_elems, 1))) return rc;
+    RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, &R, sizeof(double), cudaMemcpyHostToDevice, st));
+    if ((rc = ensure_buf(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)(n2max + 1)))) return rc;
+    if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, 1, ftype, ctx->wtab, n2max, st))) return rc;
+    wrow = ctx->wtab;
+  }
+  RG_DISPATCH_N(N, launch_debug_inverse<NN>(ctx, ctx->spec, ctx->work, wrow, d_out, st));
 }
 
 }  // namespace rg

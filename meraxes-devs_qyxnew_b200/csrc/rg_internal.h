@@ -75,49 +75,30 @@ int set_error(rg_context* ctx, int status, const std::string& msg);
       return ::rg::set_error((ctx), RG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-// Grids processed by the fused HII pipeline.
-enum HiiGrid { HG_DELTAX = 0, HG_STARS = 1, HG_XE = 2, HG_BHM = 3, HG_WSFR = 4, HG_COUNT = 5 };
-
-// Per-radius constants of the barrier test (find_HII_bubbles.c:427-442).
-struct HiiRadius {
-  double fcoll_pref;
-  float J_aux, J_aux_bh;
-  int last;
-  int first;
-  int wtab_row;        // row of the window table, -1 = unfiltered
-};
-
+// Per-snapshot constants of the barrier test.
 struct HiiConst {
   float redshift, TK, cT_ad;
   int uvb, spin, bh;
 };
 
-constexpr int HII_NSUM = 9;   // final-pass sums
+constexpr int HII_NSUM = 9;   // closing-pass sums
+constexpr int KB_MAX = 16;    // radii per batch
 
-// Launchers implemented in rg_hii.cu (dispatch on N at run time).
-int hii_forward(rg_context* ctx, int n, const float* const* d_real_padded, cf* const* d_spec, int ngrids,
+// Forward r2c of ng padded real grids into spectra spec_base + g * stride, scaled.
+int fft_forward(rg_context* ctx, int n, const float* const* d_real, int ng, cf* spec_base, size_t stride,
                 double scale, cudaStream_t st);
-int hii_window_table(rg_context* ctx, int n, double box, const double* radii, int nr, int ftype, float* d_wtab,
-                     int n2max, cudaStream_t st);
-int hii_inverse_xy(rg_context* ctx, int n, cf* const* d_spec, cf* const* d_work, int ngrids, const float* d_wrow,
-                   cudaStream_t st);
-struct HiiState {
-  float* xH;
-  float* z_in;
-  float* J21;
-  float* temp;
-  const float* Tk_box;
-  const float* deltax_unf;   // padded
-  const float* wsfr;         // padded
-  const float* bhar;         // padded, may be null
-  double* partials;          // [nblocks][HII_NSUM]
-};
-int hii_inverse_z_test(rg_context* ctx, int n, cf* const* d_work, int ngrids, const HiiRadius& r, const HiiConst& c,
-                       const HiiState& s, bool final_pass, cudaStream_t st, int* nblocks_out);
-int hii_reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out,
-                        cudaStream_t st);
-int debug_inverse_to_padded(rg_context* ctx, int n, cf* d_spec, cf* d_work, const float* d_wrow, float* d_out,
-                            cudaStream_t st);
+// W[r][n2] for the radii in d_radii (filter() closed forms, double precision)
+int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int ftype, float* d_wtab, int n2max,
+                 cudaStream_t st);
+// The excursion-set step on device grids (rg_hii.cu).
+int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out);
+// Forward + (windowed) inverse of one padded grid, for tests.
+int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype);
+int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out, cudaStream_t st);
+double* ensure_partials(rg_context* ctx, size_t n);
+int ensure_tables(rg_context* ctx, const rg_params* p);
+int validate_common(rg_context* ctx, const rg_params* p);
+
 int twiddles_for(rg_context* ctx, int n, const cf** out);
 
 // Per-kernel event timing (active when ctx->prof_on).  prof_begin records a start event on
@@ -139,10 +120,13 @@ struct rg_context {
   std::string last_error;
   // twiddle tables keyed by transform length
   std::vector<std::pair<int, rg::cf*>> twiddles;
-  // unfiltered spectra and per-radius work buffers (complex, [N/2+1][N][N])
-  rg::cf* spec[rg::HG_COUNT] = {nullptr};
-  rg::cf* work[rg::HG_COUNT] = {nullptr};
+  // unfiltered spectra [grid][N/2+1][N][N] and per-radius work buffers [radius][grid][...]
+  rg::cf* spec = nullptr;
   size_t spec_elems = 0;
+  rg::cf* work = nullptr;
+  size_t work_elems = 0;
+  uint32_t* bits = nullptr;      // packed per-cell state of the radius batches
+  size_t bits_elems = 0;
   float* wtab = nullptr;         // window table [nR][n2max+1]
   size_t wtab_elems = 0;
   double* partials = nullptr;

@@ -1,26 +1,29 @@
 // The 3-D r2c / c2r FFT passes over the spectrum layout S[kz][x][y] (complex, kz in [0, N/2],
 // x and y in [0, N)), built on line_fft:
 //
-//   k_fwd_z   : r2c along z of a padded real grid, two neighbouring rows per complex line,
-//               split into the two Hermitian halves in shared memory and stored as S[kz][x][y]
-//   k_pass_y  : c2c along y (contiguous lines), in place
-//   k_pass_x  : c2c along x (lines of stride N); a load hook (window, combination of several
-//               spectra) and a scale on store
-//   k_inv_z   : c2r along z of NG grids for a block of rows; two neighbouring rows of one grid
-//               share a complex line; the real rows land in shared memory and an epilogue
-//               object consumes them cell by cell
+//   k_fwd_z     : r2c along z of padded real grids, two neighbouring rows per complex line,
+//                 split into the two Hermitian halves in shared memory, stored as S[kz][x][y]
+//   k_pass_y    : c2c along y (contiguous lines), in place, over a run of equally spaced grids
+//   k_pass_x_fwd: c2c along x (lines of stride N), in place, scaled on store
+//   zfront      : c2r along z of NG grids for a block of rows; two neighbouring rows of one grid
+//                 share a complex line; the real rows land in shared memory for an epilogue
 //
 // Thread mappings follow the memory layout: along contiguous lines (z rows of the real grid,
 // y lines of S) consecutive threads take consecutive positions; across strided lines (x and
 // kz) consecutive threads take consecutive lines, so every global access is a run of
-// consecutive elements.
+// consecutive elements.  Exchange buffers are padded so the Stockham write pattern (stride R
+// between threads) does not collide on shared-memory banks.
 #pragma once
 
 #include "rg_fft.cuh"
 
 namespace rg {
 
-constexpr int MAXG = 8;  // grids per launch
+constexpr int MAXG = 8;  // separately addressed grids per launch
+
+// minimum resident blocks per SM for a block of n threads: enough for 512 threads, which caps
+// the registers a pass kernel may take at 128 per thread
+#define RG_MINB(n) ((n) >= 512 ? 1 : 512 / (n))
 
 struct GridPtrs {
   const void* p[MAXG];
@@ -29,42 +32,77 @@ struct GridPtrsW {
   void* p[MAXG];
 };
 
+// pointer g of a pack without dynamic indexing into kernel parameters (which would put the
+// pack in local memory)
+__device__ __forceinline__ const void* pick(const GridPtrs& a, int g) {
+  const void* r = a.p[0];
+#pragma unroll
+  for (int i = 1; i < MAXG; ++i)
+    if (g == i) r = a.p[i];
+  return r;
+}
+
 // largest power of two <= cap that divides n (at least 1)
 __host__ __device__ constexpr int pow2_div(int n, int cap) {
   int b = 1;
   while (b * 2 <= cap && n % (b * 2) == 0) b *= 2;
   return b;
 }
+__host__ __device__ constexpr int round_up(int a, int m) { return (a + m - 1) / m * m; }
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 template <int N>
 struct Cfg {
   static constexpr int T = Plan<N>::T;
+  static constexpr int V = N / T;
   static constexpr int NZ = N / 2 + 1;
   static constexpr int PADW = 2 * (N / 2 + 1);
   // x pass: BX contiguous y columns per block (>= 8 for 64-byte runs)
-  static constexpr int BX = pow2_div(N, (256 / T) >= 8 ? 256 / T : 8);
+  static constexpr int BX = pow2_div(N, cmax(256 / T, 8));
   // y pass: BY lines per block
-  static constexpr int BY = pow2_div(N, (256 / T) >= 1 ? 256 / T : 1);
+  static constexpr int BY = pow2_div(N, cmax(256 / T, 1));
   // forward z: QF row pairs per block
-  static constexpr int QF = pow2_div(N / 2, (256 / T) >= 1 ? 256 / T : 1);
-  // inverse z: QZ row pairs per block (2 QZ rows)
-  static constexpr int QZ = pow2_div(N / 2, (256 / T) >= 4 ? 256 / T : 4);
-  static constexpr int PITCH_Y = N + (T < 16 ? T : 0);   // line pitch of the y exchange buffer
-  static constexpr int PITCH_F = N + (T < 16 ? T : 0);
-  static constexpr int RT_PITCH = N + 1;                  // real row pitch (floats) in k_inv_z
+  static constexpr int QF = pow2_div(N / 2, cmax(256 / T, 1));
+  // inverse z: QZ row pairs per block (2 QZ rows), at least 4 pairs for 64-byte runs
+  static constexpr int QZ = pow2_div(N / 2, cmax(128 / T, 4));
+  // padded line pitch for position-major exchange buffers (see pos_addr)
+  static constexpr int PITCH_P = round_up(N + N / 16, 16) + (T < 16 ? T : 0);
+  static constexpr int RT_PITCH = N + 1;  // real row pitch (floats) in zfront
 };
+
+// exchange-buffer index of position p of line b when threads walk positions (one pad slot
+// every 16 positions breaks the stride-R write pattern of the first stages)
+template <int N>
+__device__ __forceinline__ int pos_addr(int b, int p) {
+  return b * Cfg<N>::PITCH_P + p + (p >> 4);
+}
+// exchange-buffer index when threads walk lines (B consecutive lines per position).  With
+// B < 16 a half-warp spans 16/B threads of the first stage, whose outputs sit R0 positions
+// apart; B extra slots after every R0 positions shift them onto different banks.
+template <int N, int B>
+__device__ __forceinline__ int line_addr(int p, int b) {
+  constexpr int R0 = Plan<N>::R[0];
+  if constexpr (B < 16) return p * B + b + B * (p / R0);
+  return p * B + b;
+}
+template <int N, int B>
+__host__ __device__ constexpr int line_buf() {
+  constexpr int R0 = Plan<N>::R[0];
+  return N * B + (B < 16 ? B * (N / R0 + 1) : 0);
+}
 
 // ---------------------------------------------------------------------------
 
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF) k_fwd_z(GridPtrs srcs, GridPtrsW dsts, const cf* __restrict__ g_tw) {
-  constexpr int T = Cfg<N>::T, Q = Cfg<N>::QF, NZ = Cfg<N>::NZ, PADW = Cfg<N>::PADW, PI = Cfg<N>::PITCH_F;
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF, RG_MINB(Cfg<N>::T* Cfg<N>::QF))
+    k_fwd_z(GridPtrs srcs, cf* __restrict__ dst_base, size_t dst_stride, const cf* __restrict__ g_tw) {
+  constexpr int T = Cfg<N>::T, Q = Cfg<N>::QF, NZ = Cfg<N>::NZ, PADW = Cfg<N>::PADW, PI = Cfg<N>::PITCH_P;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
   cf* xbuf = smem + N;
   cf* zbuf = xbuf + Q * PI;
-  const float* src = static_cast<const float*>(srcs.p[blockIdx.z]);
-  cf* dst = static_cast<cf*>(dsts.p[blockIdx.z]);
+  const float* src = static_cast<const float*>(pick(srcs, blockIdx.z));
+  cf* dst = dst_base + blockIdx.z * dst_stride;
   const int x = blockIdx.y;
   const int y0 = blockIdx.x * 2 * Q;
   const int t = threadIdx.x % T, q = threadIdx.x / T;
@@ -72,15 +110,15 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF) k_fwd_z(GridPtrs srcs, 
   __syncthreads();
   const float* r0 = src + ((size_t)x * N + y0 + 2 * q) * PADW;
   line_fft<N, false>(
-      t, xbuf, s_tw, [&](int p) { return cf{__ldg(r0 + p), __ldg(r0 + PADW + p)}; },
-      [&](int p) { return q * PI + p; }, [&](int p, cf v) { zbuf[q * PI + p] = v; });
+      t, xbuf, s_tw, [&](int p, int) { return cf{__ldg(r0 + p), __ldg(r0 + PADW + p)}; },
+      [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v) { zbuf[pos_addr<N>(q, p)] = v; });
   __syncthreads();
   // split Z = X(y) + i X(y+1) and store S[k][x][y0 .. y0 + 2Q)
   for (int i = threadIdx.x; i < NZ * 2 * Q; i += T * Q) {
     const int yy = i % (2 * Q), k = i / (2 * Q);
     const int qq = yy >> 1;
-    const cf zk = zbuf[qq * PI + k];
-    const cf zn = zbuf[qq * PI + (N - k) % N];
+    const cf zk = zbuf[pos_addr<N>(qq, k)];
+    const cf zn = zbuf[pos_addr<N>(qq, (N - k) % N)];
     cf out;
     if ((yy & 1) == 0) {
       out = cf{0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y)};  // (Z[k] + conj Z[N-k]) / 2
@@ -91,13 +129,15 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF) k_fwd_z(GridPtrs srcs, 
   }
 }
 
+// y pass over grids base + z * stride (z = blockIdx.z), in place
 template <int N, bool INV>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BY) k_pass_y(GridPtrsW bufs, const cf* __restrict__ g_tw) {
-  constexpr int T = Cfg<N>::T, B = Cfg<N>::BY, PI = Cfg<N>::PITCH_Y;
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BY, RG_MINB(Cfg<N>::T* Cfg<N>::BY))
+    k_pass_y(cf* __restrict__ base, size_t stride, const cf* __restrict__ g_tw) {
+  constexpr int T = Cfg<N>::T, B = Cfg<N>::BY;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
   cf* xbuf = smem + N;
-  cf* g = static_cast<cf*>(bufs.p[blockIdx.z]);
+  cf* g = base + blockIdx.z * stride;
   const int kz = blockIdx.y;
   const int x0 = blockIdx.x * B;
   const int t = threadIdx.x % T, b = threadIdx.x / T;
@@ -105,66 +145,32 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BY) k_pass_y(GridPtrsW bufs
   __syncthreads();
   cf* line = g + ((size_t)kz * N + x0 + b) * N;
   line_fft<N, INV>(
-      t, xbuf, s_tw, [&](int p) { return line[p]; }, [&](int p) { return b * PI + p; },
+      t, xbuf, s_tw, [&](int p, int) { return line[p]; }, [&](int p) { return pos_addr<N>(b, p); },
       [&](int p, cf v) { line[p] = v; });
 }
 
-// x pass.  Load hook LD(line_ptr_offset, p, y, kz) -> cf supplies the input (plain copy,
-// window, combination of spectra); the result is scaled by `scale` and stored to dst.
-template <int N, bool INV, class LD>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX) k_pass_x(LD ld, GridPtrsW dsts, const cf* __restrict__ g_tw, float scale) {
+// forward x pass over grids base + z * stride, in place, scaled on store
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<N>::BX))
+    k_pass_x_fwd(cf* __restrict__ base, size_t stride, const cf* __restrict__ g_tw, float scale) {
   constexpr int T = Cfg<N>::T, B = Cfg<N>::BX;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
   cf* xbuf = smem + N;
-  const int g = blockIdx.z;
-  cf* dst = static_cast<cf*>(dsts.p[g]);
+  cf* g = base + blockIdx.z * stride;
   const int kz = blockIdx.y;
-  const int y0 = blockIdx.x * B;
   const int b = threadIdx.x % B, t = threadIdx.x / B;
-  const int y = y0 + b;
+  const size_t col = (size_t)kz * N * N + blockIdx.x * B + b;
   load_twiddles<N>(s_tw, g_tw);
   __syncthreads();
-  const size_t col = (size_t)kz * N * N + y;   // element (kz, p, y) at col + p * N
-  line_fft<N, INV>(
-      t, xbuf, s_tw, [&](int p) { return ld(g, col + (size_t)p * N, p, y, kz); },
-      [&](int p) { return p * B + b; },
-      [&](int p, cf v) {
-        v.x *= scale;
-        v.y *= scale;
-        dst[col + (size_t)p * N] = v;
-      });
+  line_fft<N, false>(
+      t, xbuf, s_tw, [&](int p, int) { return g[col + (size_t)p * N]; }, [&](int p) { return line_addr<N, B>(p, b); },
+      [&](int p, cf v) { g[col + (size_t)p * N] = cf{v.x * scale, v.y * scale}; });
 }
 
-// plain x-pass input: src[g][idx]
-struct LoadPlain {
-  GridPtrs src;
-  __device__ __forceinline__ cf operator()(int g, size_t idx, int, int, int) const {
-    return static_cast<const cf*>(src.p[g])[idx];
-  }
-};
-
-// x-pass input multiplied by a window that depends on |k|^2 = nx^2 + ny^2 + nz^2
-template <int N>
-struct LoadWindow {
-  GridPtrs src;
-  const float* wrow;   // W[n2], null = no window
-  __device__ __forceinline__ cf operator()(int g, size_t idx, int p, int y, int kz) const {
-    cf v = static_cast<const cf*>(src.p[g])[idx];
-    if (wrow != nullptr) {
-      const int nx = p > N / 2 ? p - N : p;
-      const int ny = y > N / 2 ? y - N : y;
-      const float w = __ldg(wrow + nx * nx + ny * ny + kz * kz);
-      v.x *= w;
-      v.y *= w;
-    }
-    return v;
-  }
-};
-
 // ---------------------------------------------------------------------------
-// inverse z: c2r of NG grids for rows [y0, y0 + 2 QZ) of plane x.  Real row r of grid g lands
-// at rt[(g * 2 QZ + r) * RT_PITCH + z]; then epi(rt, x, y0) consumes the block's cells.
+// zfront: c2r of NG grids (work + g * stride) for rows [y0, y0 + 2 QZ) of plane x.  Real row
+// r of grid g lands at rt[(g * 2 QZ + r) * RT_PITCH + z].  Ends with a block barrier.
 
 template <int N>
 __device__ __forceinline__ cf build_c2r_input(const cf* __restrict__ g, size_t colpair, int p) {
@@ -177,46 +183,50 @@ __device__ __forceinline__ cf build_c2r_input(const cf* __restrict__ g, size_t c
   return cf{ab.x + ab.w, ab.z - ab.y};
 }
 
-template <int N, int NG, class EPI>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ) k_inv_z(GridPtrs works, const cf* __restrict__ g_tw, EPI epi) {
+template <int N>
+constexpr size_t zfront_smem_bytes(int ng) {
+  return sizeof(cf) * (N + (size_t)line_buf<N, Cfg<N>::QZ>()) +
+         sizeof(float) * (size_t)ng * 2 * Cfg<N>::QZ * (N + 1);
+}
+
+template <int N, int NG>
+__device__ __forceinline__ void zfront(const cf* __restrict__ work, size_t stride, const cf* s_tw, cf* xbuf,
+                                       float* rt, int x, int y0) {
   constexpr int T = Cfg<N>::T, Q = Cfg<N>::QZ, RP = Cfg<N>::RT_PITCH;
-  extern __shared__ cf smem[];
-  cf* s_tw = smem;
-  cf* xbuf = smem + N;
-  float* rt = reinterpret_cast<float*>(xbuf + N * Q);
-  const int x = blockIdx.y;
-  const int y0 = blockIdx.x * 2 * Q;
   const int q = threadIdx.x % Q, t = threadIdx.x / Q;
-  load_twiddles<N>(s_tw, g_tw);
-  __syncthreads();
   const size_t colpair = (size_t)x * N + y0 + 2 * q;
 #pragma unroll
   for (int g = 0; g < NG; ++g) {
-    const cf* src = static_cast<const cf*>(works.p[g]);
+    const cf* src = work + g * stride;
     float* r0 = rt + (size_t)(g * 2 * Q + 2 * q) * RP;
     line_fft<N, true>(
-        t, xbuf, s_tw, [&](int p) { return build_c2r_input<N>(src, colpair, p); },
-        [&](int p) { return p * Q + q; },
+        t, xbuf, s_tw, [&](int p, int) { return build_c2r_input<N>(src, colpair, p); },
+        [&](int p) { return line_addr<N, Q>(p, q); },
         [&](int p, cf v) {
           r0[p] = v.x;
           r0[RP + p] = v.y;
         });
   }
   __syncthreads();
-  epi.template run<N, 2 * Q, T * Q>(rt, x, y0);
 }
 
-// epilogue: write the real rows to a padded grid
-struct EpiPadded {
-  float* out;
-  template <int N, int ROWS, int NTH>
-  __device__ __forceinline__ void run(const float* rt, int x, int y0) const {
-    constexpr int PADW = 2 * (N / 2 + 1);
-    for (int i = threadIdx.x; i < ROWS * N; i += NTH) {
-      const int z = i % N, r = i / N;
-      out[((size_t)x * N + y0 + r) * PADW + z] = rt[r * (N + 1) + z];
-    }
+// c2r of one spectrum into a padded real grid (tests)
+template <int N>
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<N>::QZ))
+    k_inv_z_padded(const cf* __restrict__ work, const cf* __restrict__ g_tw, float* __restrict__ out) {
+  constexpr int T = Cfg<N>::T, Q = Cfg<N>::QZ, PADW = Cfg<N>::PADW;
+  extern __shared__ cf smem[];
+  cf* s_tw = smem;
+  cf* xbuf = smem + N;
+  float* rt = reinterpret_cast<float*>(xbuf + line_buf<N, Q>());
+  const int x = blockIdx.y, y0 = blockIdx.x * 2 * Q;
+  load_twiddles<N>(s_tw, g_tw);
+  __syncthreads();
+  zfront<N, 1>(work, 0, s_tw, xbuf, rt, x, y0);
+  for (int i = threadIdx.x; i < 2 * Q * N; i += T * Q) {
+    const int z = i % N, r = i / N;
+    out[((size_t)x * N + y0 + r) * PADW + z] = rt[r * (N + 1) + z];
   }
-};
+}
 
 }  // namespace rg
