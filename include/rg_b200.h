@@ -109,7 +109,8 @@ typedef struct rg_snapshot {
   int snapshot;
   int n_snapshots;
   const double* ZZ;                 /* host array, ZZ[0..n_snapshots) descending redshifts */
-  const double* stored_fcoll;       /* host array [n_snapshots]; ComputeTs writes [snapshot] */
+  double* stored_fcoll;             /* host array [n_snapshots]; rg_compute_Ts reads [snapshot - 1]
+                                       and writes [snapshot] (ComputeTs.c:662) */
 } rg_snapshot;
 
 /* Global averages the reference stores into reion_grids_t (src/meraxes.h:628-675). */
@@ -197,6 +198,17 @@ int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* 
 
 /* Radius schedule of find_HII_bubbles: fills up to max_r radii, returns the count in *n. */
 int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int max_r, int* n);
+
+/* Host-side coefficient engine of ComputeTs (no device work), for nS = TsNumFilterSteps
+   shells of snapshot s with n_hist history slots:
+     shells[6][nS] : R (Mpc), zpp_edge, zpp, dzpp, dt_dzpp, sum_lyn   (ComputeTs.c:339-478, 900-1011)
+     freq[3][14][nS]: heat, ion, lya frequency integrals per x_e node (ComputeTs.c:761-808)
+     coef[nS][1 + n_hist]: weight of source k in shell r's source grid, k = 0 this snapshot's
+                    sfr / xray_luminosity, k = 1 + h history slot h (the re-weighting of
+                    ComputeTs.c:366-478 as a linear combination)
+   freq is computed only when freq != NULL. */
+int rg_debug_ts_tables(const rg_params* p, const rg_snapshot* s, int n_hist, double x_e_ave,
+                       double collapse_fraction, int max_shells, double* shells, double* freq, float* coef);
 
 #ifdef __cplusplus
 }

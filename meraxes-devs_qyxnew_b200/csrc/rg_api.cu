@@ -10,6 +10,7 @@
 
 #include "rg_fft.cuh"
 #include "rg_internal.h"
+#include "rg_xray.h"
 
 namespace rg {
 
@@ -37,10 +38,10 @@ double hubble_time_at(const rg_params* p, double z) {
 
 double dtdz(const rg_params* p, float zf) {
   // src/core/XRayHeatingFunctions.c:426-440
-  const double z = zf;
+  const double opz = (double)(1.0f + zf);  // 1 + z is a float sum in the C
   const double oml = p->OmegaLambda, omm = p->OmegaM;
-  const double x = std::sqrt(oml / omm) * std::pow(1 + z, -3.0 / 2.0);
-  const double dxdz = std::sqrt(oml / omm) * std::pow(1 + z, -5.0 / 2.0) * (-3.0 / 2.0);
+  const double x = std::sqrt(oml / omm) * std::pow(opz, -3.0 / 2.0);
+  const double dxdz = std::sqrt(oml / omm) * std::pow(opz, -5.0 / 2.0) * (-3.0 / 2.0);
   const double const1 = 2 * std::sqrt(1 + omm / oml) / (3.0 * HUBBLE * p->Hubble_h);
   const double numer = dxdz * (1 + x * std::pow(std::pow(x, 2) + 1, -0.5));
   const double denom = x + std::sqrt(std::pow(x, 2) + 1);
@@ -307,6 +308,9 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
   if (ctx->d_radii) cudaFree(ctx->d_radii);
+  if (ctx->ts_acc) cudaFree(ctx->ts_acc);
+  if (ctx->ts_stage) cudaFree(ctx->ts_stage);
+  if (ctx->ts_const) cudaFree(ctx->ts_const);
   for (void* p : ctx->owned) cudaFree(p);
   prof_resolve(ctx);
   for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
@@ -512,6 +516,42 @@ int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* 
   return RG_OK;
 }
 
+int rg_debug_ts_tables(const rg_params* p, const rg_snapshot* s, int n_hist, double x_e_ave,
+                       double collapse_fraction, int max_shells, double* shells, double* freq, float* coef) {
+  if (!p || !s || !s->ZZ || !shells || !coef || n_hist < 0) return RG_EINVAL;
+  if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return RG_EINVAL;
+  const int nS = p->TsNumFilterSteps;
+  if (nS < 1 || nS > max_shells) return RG_EINVAL;
+  TsShells sh = ts_shells(p, s->ZZ, s->n_snapshots, s->snapshot, n_hist);
+  if (sh.error) return RG_EINVAL;
+  TsTables tb;
+  if (freq) {
+    if (!s->stored_fcoll && s->snapshot > 0) return RG_EINVAL;
+    Tables t;
+    if (!p->TablesForXHeatingDir) return RG_ETABLE;
+    if (!load_tables(p->TablesForXHeatingDir, p->ReionNionPhotPerBary, &t).empty()) return RG_ETABLE;
+    std::string msg;
+    int rc = ts_tables(p, t, sh, s->ZZ[s->snapshot], x_e_ave, collapse_fraction, s->ZZ, s->stored_fcoll,
+                       s->snapshot, &tb, &msg);
+    if (rc) return rc;
+    for (int k = 0; k < 3; ++k) {
+      const std::vector<double>& v = k == 0 ? tb.heat : k == 1 ? tb.ion : tb.lya;
+      for (int m = 0; m < x_int_NXHII; ++m)
+        for (int r = 0; r < nS; ++r) freq[((size_t)k * x_int_NXHII + m) * nS + r] = v[(size_t)m * nS + r];
+    }
+  }
+  for (int r = 0; r < nS; ++r) {
+    shells[r] = sh.R[r];
+    shells[nS + r] = sh.zpp_edge[r];
+    shells[2 * nS + r] = sh.zpp[r];
+    shells[3 * nS + r] = sh.dzpp[r];
+    shells[4 * nS + r] = sh.dt_dzpp[r];
+    shells[5 * nS + r] = freq ? tb.sum_lyn[r] : 0.0;
+    for (int k = 0; k < sh.nsrc; ++k) coef[(size_t)r * sh.nsrc + k] = sh.coef[(size_t)r * sh.nsrc + k];
+  }
+  return RG_OK;
+}
+
 int rg_profile_enable(rg_context* ctx, int on) {
   if (!ctx) return RG_EINVAL;
   prof_resolve(ctx);
@@ -529,15 +569,66 @@ int rg_profile_read(rg_context* ctx, rg_kernel_stat* out, int max, int* n) {
   return RG_OK;
 }
 
+static int compute_ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+                      const rg_grids* src_host, rg_ts_scalars* out) {
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  if (!s->ZZ) return set_error(ctx, RG_EINVAL, "ZZ is required");
+  if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return set_error(ctx, RG_EINVAL, "snapshot out of range");
+  const int N = ctx->N;
+  if (N < 8 || (N & (N - 1)) != 0)
+    return set_error(ctx, RG_EUNSUPPORTED, "ComputeTs needs a power-of-two ReionGridDim");
+  if (p->Flag_IncludeAGNXray)
+    return set_error(ctx, RG_EUNSUPPORTED, "Flag_IncludeAGNXray=1 (AGN X-ray channels) is not implemented");
+  if (p->TsHeatingFilterType < 0 || p->TsHeatingFilterType > 2)
+    return set_error(ctx, RG_EINVAL, "TsHeatingFilterType must be 0, 1 or 2");
+  if (p->TsNumFilterSteps < 1 || p->TsNumFilterSteps > 1024)
+    return set_error(ctx, RG_EINVAL, "TsNumFilterSteps must be in [1, 1024]");
+  if (!g->deltax || !g->stars || !g->x_e_box_prev || !g->x_e_box || !g->Tk_box || !g->TS_box)
+    return set_error(ctx, RG_EINVAL, "missing grid pointer");
+  const rg_grids* sg = src_host ? src_host : g;
+  if (sg->n_hist < 0 || (sg->n_hist > 0 && (!sg->sfr_histories || !sg->xray_luminosity_histories)))
+    return set_error(ctx, RG_EINVAL, "n_hist > 0 needs sfr_histories and xray_luminosity_histories");
+  const bool homog = (s->ZZ[s->snapshot] - p->ReionMaxHeatingRedshift) >= -0.0001;
+  if (!homog && (!sg->sfr || !sg->xray_luminosity))
+    return set_error(ctx, RG_EINVAL, "ComputeTs needs the sfr and xray_luminosity grids");
+  if ((rc = ensure_tables(ctx, p))) return rc;
+  cudaSetDevice(ctx->device);
+  rc = ts_snapshot(ctx, p, s, g, out, src_host);
+  if (rc == RG_OK && s->stored_fcoll) s->stored_fcoll[s->snapshot] = out->collapse_fraction;
+  return rc;
+}
+
 int rg_compute_Ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_ts_scalars* out) {
-  (void)p; (void)s; (void)g; (void)out;
-  return set_error(ctx, RG_EUNSUPPORTED, "rg_compute_Ts is not built yet");
+  if (!ctx || !p || !s || !g || !out) return RG_EINVAL;
+  return compute_ts(ctx, p, s, g, nullptr, out);
 }
 
 int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* h,
                        rg_ts_scalars* out) {
-  (void)p; (void)s; (void)h; (void)out;
-  return set_error(ctx, RG_EUNSUPPORTED, "rg_compute_Ts_host is not built yet");
+  if (!ctx || !p || !s || !h || !out) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  if (!p->Flag_IncludeSpinTemp) return set_error(ctx, RG_EINVAL, "rg_compute_Ts_host needs Flag_IncludeSpinTemp=1");
+  cudaSetDevice(ctx->device);
+  if ((rc = ensure_dev_grids(ctx, p, 0))) return rc;
+  const rg_grids& d = ctx->dev_grids;
+  const size_t n = (size_t)ctx->N;
+  const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float), br = n * n * n * sizeof(float);
+  const auto H2D = cudaMemcpyHostToDevice;
+  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D))) return rc;
+  if ((rc = copy_grid(ctx, d.x_e_box_prev, h->x_e_box_prev, bp, H2D))) return rc;
+  if ((rc = copy_grid(ctx, d.Tk_box, h->Tk_box, br, H2D))) return rc;
+  // the source grids are staged from h inside the step (only the history slots in use)
+  if ((rc = compute_ts(ctx, p, s, &d, h, out))) return rc;
+  const auto D2H = cudaMemcpyDeviceToHost;
+  if ((rc = copy_grid(ctx, h->x_e_box_prev, d.x_e_box_prev, bp, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->x_e_box, d.x_e_box, bp, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->Tk_box, d.Tk_box, br, D2H))) return rc;
+  if ((rc = copy_grid(ctx, h->TS_box, d.TS_box, br, D2H))) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
 }
 
 }  // extern "C"

@@ -144,61 +144,77 @@ __device__ __forceinline__ void dft_small(cf* v) {
 }
 
 // ---------------------------------------------------------------------------
-// radix plans: stages R[0..S) and threads per line T (T divides every N / R[s])
+// radix plans: length NN, stages R[0..S) and threads per line T (T divides every N / R[s])
 
-template <int N>
-struct Plan;
-#define RG_PLAN(n, t, ...)                       \
-  template <>                                    \
-  struct Plan<n> {                               \
-    static constexpr int T = t;                  \
-    static constexpr int R[] = {__VA_ARGS__};    \
+#define RG_PLAN(name, n, t, ...)                      \
+  template <>                                         \
+  struct name<n> {                                    \
+    static constexpr int NN = n;                      \
+    static constexpr int T = t;                       \
+    static constexpr int R[] = {__VA_ARGS__};         \
     static constexpr int S = sizeof(R) / sizeof(int); \
   };
-RG_PLAN(8, 1, 8)
-RG_PLAN(16, 1, 16)
-RG_PLAN(24, 1, 8, 3)
-RG_PLAN(32, 4, 8, 4)
-RG_PLAN(48, 2, 8, 2, 3)
-RG_PLAN(64, 8, 8, 8)
-RG_PLAN(96, 4, 8, 4, 3)
-RG_PLAN(128, 8, 16, 8)
-RG_PLAN(192, 8, 8, 8, 3)
-RG_PLAN(256, 16, 16, 16)
-RG_PLAN(384, 16, 8, 8, 2, 3)
-RG_PLAN(512, 64, 8, 8, 8)
+
+// default plans: few stages (one shared-memory exchange where the radices allow)
+template <int N>
+struct Plan;
+RG_PLAN(Plan, 8, 1, 8)
+RG_PLAN(Plan, 16, 1, 16)
+RG_PLAN(Plan, 24, 1, 8, 3)
+RG_PLAN(Plan, 32, 4, 8, 4)
+RG_PLAN(Plan, 48, 2, 8, 2, 3)
+RG_PLAN(Plan, 64, 8, 8, 8)
+RG_PLAN(Plan, 96, 4, 8, 4, 3)
+RG_PLAN(Plan, 128, 8, 16, 8)
+RG_PLAN(Plan, 192, 8, 8, 8, 3)
+RG_PLAN(Plan, 256, 16, 16, 16)
+RG_PLAN(Plan, 384, 16, 8, 8, 2, 3)
+RG_PLAN(Plan, 512, 64, 8, 8, 8)
+
+// eight values per thread (power-of-two N): leaves registers for per-cell accumulators
+template <int N>
+struct Plan8;
+RG_PLAN(Plan8, 8, 1, 8)
+RG_PLAN(Plan8, 16, 2, 8, 2)
+RG_PLAN(Plan8, 32, 4, 8, 4)
+RG_PLAN(Plan8, 64, 8, 8, 8)
+RG_PLAN(Plan8, 128, 16, 8, 4, 4)
+RG_PLAN(Plan8, 256, 32, 8, 8, 4)
+RG_PLAN(Plan8, 512, 64, 8, 8, 8)
 #undef RG_PLAN
 
-template <int N, int s>
+template <class PL, int s>
 struct StageNS {
-  static constexpr int value = StageNS<N, s - 1>::value * Plan<N>::R[s - 1];
+  static constexpr int value = StageNS<PL, s - 1>::value * PL::R[s - 1];
 };
-template <int N>
-struct StageNS<N, 0> {
+template <class PL>
+struct StageNS<PL, 0> {
   static constexpr int value = 1;
 };
 
-template <int N>
+template <class PL>
 constexpr int plan_product() {
   int p = 1;
-  for (int i = 0; i < Plan<N>::S; ++i) p *= Plan<N>::R[i];
+  for (int i = 0; i < PL::S; ++i) p *= PL::R[i];
   return p;
 }
 
 // Stage-0 input position of register slot `slot` (0 <= slot < N/T) of thread t.
-template <int N>
+template <class PL>
 __device__ __forceinline__ int stage0_pos(int t, int slot) {
-  constexpr int R = Plan<N>::R[0];
-  constexpr int T = Plan<N>::T;
+  constexpr int R = PL::R[0];
+  constexpr int T = PL::T;
+  constexpr int N = PL::NN;
   return t + (slot / R) * T + (slot % R) * (N / R);
 }
 
 // run stage s: fill v from `load(pos, slot)`, twiddle, DFT
-template <int N, int s, bool INV, class Load>
+template <class PL, int s, bool INV, class Load>
 __device__ __forceinline__ void stage_compute(cf* v, int t, const cf* __restrict__ tw, Load&& load) {
-  constexpr int T = Plan<N>::T;
-  constexpr int R = Plan<N>::R[s];
-  constexpr int NS = StageNS<N, s>::value;
+  constexpr int N = PL::NN;
+  constexpr int T = PL::T;
+  constexpr int R = PL::R[s];
+  constexpr int NS = StageNS<PL, s>::value;
   constexpr int K = (N / R) / T;
   static_assert((N / R) % T == 0, "T must divide N/R");
 #pragma unroll
@@ -219,48 +235,70 @@ __device__ __forceinline__ void stage_compute(cf* v, int t, const cf* __restrict
   }
 }
 
-// hand stage s's outputs to `put(pos, value)`
-template <int N, int s, class Put>
+// hand stage s's outputs to `put(pos, value, slot)`
+template <class PL, int s, class Put>
 __device__ __forceinline__ void stage_emit(const cf* v, int t, Put&& put) {
-  constexpr int T = Plan<N>::T;
-  constexpr int R = Plan<N>::R[s];
-  constexpr int NS = StageNS<N, s>::value;
+  constexpr int T = PL::T;
+  constexpr int N = PL::NN;
+  constexpr int R = PL::R[s];
+  constexpr int NS = StageNS<PL, s>::value;
   constexpr int K = (N / R) / T;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int j = t + k * T;
     const int idxD = (j / NS) * NS * R + (j % NS);
 #pragma unroll
-    for (int r = 0; r < R; ++r) put(idxD + r * NS, v[k * R + r]);
+    for (int r = 0; r < R; ++r) put(idxD + r * NS, v[k * R + r], k * R + r);
   }
 }
 
-template <int N, int s, bool INV, class Addr, class Store>
+template <class PL, int s, bool INV, class Addr, class Store>
 __device__ __forceinline__ void stages_from(cf* v, int t, cf* xbuf, Addr&& addr, const cf* tw, Store&& store) {
-  if constexpr (s + 1 < Plan<N>::S) {
+  if constexpr (s + 1 < PL::S) {
     __syncthreads();  // every thread is done reading xbuf
-    stage_emit<N, s>(v, t, [&](int p, cf x) { xbuf[addr(p)] = x; });
+    stage_emit<PL, s>(v, t, [&](int p, cf x, int) { xbuf[addr(p)] = x; });
     __syncthreads();
-    stage_compute<N, s + 1, INV>(v, t, tw, [&](int p, int) { return xbuf[addr(p)]; });
-    stages_from<N, s + 1, INV>(v, t, xbuf, addr, tw, store);
+    stage_compute<PL, s + 1, INV>(v, t, tw, [&](int p, int) { return xbuf[addr(p)]; });
+    stages_from<PL, s + 1, INV>(v, t, xbuf, addr, tw, store);
   } else {
-    stage_emit<N, s>(v, t, store);
+    stage_emit<PL, s>(v, t, store);
   }
 }
 
-// Full transform of one line by thread t (0 <= t < Plan<N>::T):
-//   load(p, slot)  -> input element at position p, held in register slot `slot`
-//                     (stage0_pos<N>(t, slot) == p)
-//   addr(p)        -> index into xbuf of position p of this thread's line (exchange buffer)
-//   store(p, val)  <- output element at position p
+// Last-stage output position of register slot `slot` of thread t (the order store() sees).
+template <class PL>
+__device__ __forceinline__ int last_pos(int t, int slot) {
+  constexpr int s = PL::S - 1;
+  constexpr int R = PL::R[s];
+  constexpr int NS = StageNS<PL, s>::value;
+  const int j = t + (slot / R) * PL::T;
+  return (j / NS) * NS * R + (j % NS) + (slot % R) * NS;
+}
+
+// Full transform of one line by thread t (0 <= t < PL::T):
+//   load(p, slot)       -> input element at position p, held in register slot `slot`
+//                          (stage0_pos<PL>(t, slot) == p)
+//   addr(p)             -> index into xbuf of position p of this thread's line (exchange buffer)
+//   store(p, val, slot) <- output element at position p (last_pos<PL>(t, slot) == p)
 // Every thread of the block must call it (it contains block barriers when S > 1).
+template <class PL, bool INV, class Load, class Addr, class Store>
+__device__ __forceinline__ void line_fft_p(int t, cf* xbuf, const cf* tw, Load&& load, Addr&& addr, Store&& store) {
+  static_assert(plan_product<PL>() == PL::NN, "radix plan does not multiply to N");
+  constexpr int V = PL::NN / PL::T;
+  cf v[V];
+  stage_compute<PL, 0, INV>(v, t, tw, load);
+  stages_from<PL, 0, INV>(v, t, xbuf, addr, tw, store);
+}
+
+// line_fft with the default plan; store(p, val) without the slot
 template <int N, bool INV, class Load, class Addr, class Store>
 __device__ __forceinline__ void line_fft(int t, cf* xbuf, const cf* tw, Load&& load, Addr&& addr, Store&& store) {
-  static_assert(plan_product<N>() == N, "radix plan does not multiply to N");
-  constexpr int V = N / Plan<N>::T;
-  cf v[V];
-  stage_compute<N, 0, INV>(v, t, tw, load);
-  stages_from<N, 0, INV>(v, t, xbuf, addr, tw, store);
+  line_fft_p<Plan<N>, INV>(t, xbuf, tw, load, addr, [&](int p, cf v, int) { store(p, v); });
+}
+
+template <int N>
+__device__ __forceinline__ int stage0_pos(int t, int slot) {
+  return stage0_pos<Plan<N>>(t, slot);
 }
 
 // Copy the N-entry twiddle table into shared memory (caller syncs).

@@ -92,6 +92,11 @@ int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int
                  cudaStream_t st);
 // The excursion-set step on device grids (rg_hii.cu).
 int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out);
+// The spin-temperature step on device grids (rg_ts.cu).  With src_host, the sfr /
+// xray_luminosity grids and their histories are read from those HOST arrays instead of g, and
+// only the history slots the shells use are copied to the device.
+int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_ts_scalars* out,
+                const rg_grids* src_host = nullptr);
 // Forward + (windowed) inverse of one padded grid, for tests.
 int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype);
 int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out, cudaStream_t st);
@@ -142,6 +147,12 @@ struct rg_context {
   rg::Tables tables;
   double* d_radii = nullptr;     // device copy of the radius list
   size_t d_radii_elems = 0;
+  double* ts_acc = nullptr;      // ComputeTs per-cell FP64 shell sums [4][N^3]
+  size_t ts_acc_elems = 0;
+  float* ts_stage = nullptr;     // ComputeTs source grids staged from host memory [slot][2][padded]
+  size_t ts_stage_elems = 0;
+  char* ts_const = nullptr;      // ComputeTs device constants and per-batch coefficients
+  size_t ts_const_elems = 0;
   // profiling
   bool prof_on = false;
   struct ProfRec {

@@ -90,6 +90,16 @@ __host__ __device__ constexpr int line_buf() {
   constexpr int R0 = Plan<N>::R[0];
   return N * B + (B < 16 ? B * (N / R0 + 1) : 0);
 }
+// the same for a plan whose first radix is R0
+template <int R0, int B>
+__device__ __forceinline__ int line_addr_r0(int p, int b) {
+  if constexpr (B < 16) return p * B + b + B * (p / R0);
+  return p * B + b;
+}
+template <int N, int R0, int B>
+__host__ __device__ constexpr int line_buf_r0() {
+  return N * B + (B < 16 ? B * (N / R0 + 1) : 0);
+}
 
 // ---------------------------------------------------------------------------
 

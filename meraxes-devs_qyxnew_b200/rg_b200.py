@@ -114,6 +114,8 @@ _SIGS = {
     "rg_delta_T_host": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_snapshot), _P(rg_grids), _P(C.c_double)]),
     "rg_debug_filter_roundtrip": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_void_p, C.c_double, C.c_int]),
     "rg_radius_schedule": (C.c_int, [_P(rg_params), C.c_double, _P(C.c_double), C.c_int, _P(C.c_int)]),
+    "rg_debug_ts_tables": (C.c_int, [_P(rg_params), _P(rg_snapshot), C.c_int, C.c_double, C.c_double, C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
@@ -156,6 +158,22 @@ def make_params(n: int, box: float, **kw) -> rg_params:
             raise AttributeError(k)
         setattr(p, k, v)
     return p
+
+
+def ts_tables(p: rg_params, zz, snap: int, n_hist: int, x_e_ave: float, collapse_fraction: float,
+              stored_fcoll=None, with_freq: bool = True):
+    """The host coefficient engine of the spin-temperature step (no device work): returns
+    (shells[6][nS], freq[3][14][nS] or None, coef[nS][1 + n_hist])."""
+    import numpy as np
+    ns = p.TsNumFilterSteps
+    shells = np.zeros((6, ns))
+    freq = np.zeros((3, 14, ns)) if with_freq else None
+    coef = np.zeros((ns, 1 + n_hist), np.float32)
+    s = snapshot(zz, snap, stored_fcoll)
+    check(None, load().rg_debug_ts_tables(C.byref(p), C.byref(s), n_hist, x_e_ave, collapse_fraction, ns,
+                                          shells.ctypes.data, freq.ctypes.data if with_freq else None,
+                                          coef.ctypes.data))
+    return shells, freq, coef
 
 
 def snapshot(zz, snap: int, stored_fcoll=None):

@@ -153,3 +153,36 @@ CONFIGS = {
     # full step at 512^3, 500 Mpc/h, z=8, R0 = 0.62*L (about 60 radii), then Ts and delta_T
     "c4_512": GridConfig("c4_512", 512, 500.0, 8.0, r_bubble_max=1000.0, spin_temp=1, seed=1813),
 }
+
+
+@dataclasses.dataclass
+class TsInputs:
+    """Spin-temperature inputs besides the source grids (all padded float32 unless noted)."""
+    x_e_box_prev: np.ndarray
+    Tk_box: np.ndarray                 # real [N]^3
+    sfr_histories: list                # slot h = snapshot (current - h)
+    xray_histories: list
+    stored_fcoll: np.ndarray           # float64 [n_snapshots]
+
+
+def make_ts_inputs(src: SourceGrids, zz: np.ndarray, snap: int, n_hist: int, seed: int,
+                   fcoll_prev: float = 1e-5) -> TsInputs:
+    """Synthetic ComputeTs state: x_e ~ 2e-4 LN(0, 0.3), T_K ~ 12 K (1 + 0.3 delta) floored at
+    2 K, and SFR / X-ray histories that decay towards higher redshift as exp(-0.4 (z_h - z))
+    with a per-slot LN(0, 0.2) cell modulation (slot 0 is this snapshot's grids)."""
+    rng = np.random.default_rng(seed)
+    n = src.n
+    d = from_padded(src.deltax).astype(np.float64)
+    xe = 2e-4 * rng.lognormal(0.0, 0.3, size=d.shape)
+    tk = np.maximum(12.0 * (1.0 + 0.3 * d), 2.0).astype(np.float32)
+    sfr_h, xr_h = [src.sfr.copy()], [src.xray.copy()]
+    for h in range(1, n_hist):
+        zh = zz[snap - h] if snap - h >= 0 else zz[0]
+        mod = rng.lognormal(0.0, 0.2, size=d.shape) * math.exp(-0.4 * (zh - zz[snap]))
+        sfr_h.append(to_padded(from_padded(src.sfr) * mod))
+        xr_h.append(to_padded(from_padded(src.xray) * mod))
+    sf = np.zeros(len(zz))
+    if snap > 0:
+        sf[snap - 1] = fcoll_prev
+    return TsInputs(x_e_box_prev=to_padded(xe), Tk_box=tk, sfr_histories=sfr_h, xray_histories=xr_h,
+                    stored_fcoll=sf)

@@ -85,6 +85,15 @@ class Params:
     Flag_IncludeSpinTemp: int = 0
     Flag_IncludeRecombinations: int = 0
     Flag_BHFeedback: int = 0
+    # ComputeTs (input/params/defaults.par)
+    TsHeatingFilterType: int = 1
+    TsNumFilterSteps: int = 40
+    Flag_IncludeAGNXray: int = 0
+    ReionMaxHeatingRedshift: float = 30.0
+    NuXrayThreshold: float = 500.0
+    NuXraySoftCut: float = 2000.0
+    NuXrayMax: float = 10000.0
+    SpecIndexXrayGal: float = 1.0
 
 
 @dataclasses.dataclass
@@ -114,10 +123,10 @@ def hubble_time(p: Params, z: float) -> float:
 
 def dtdz(p: Params, z: float) -> float:
     """src/core/XRayHeatingFunctions.c:426-440 (float argument as in the C)."""
-    z = float(np.float32(z))
+    opz = float(np.float32(1) + np.float32(z))       # 1 + z is a float sum in the C
     oml, omm = p.OmegaLambda, p.OmegaM
-    x = math.sqrt(oml / omm) * (1 + z) ** (-1.5)
-    dxdz = math.sqrt(oml / omm) * (1 + z) ** (-2.5) * (-1.5)
+    x = math.sqrt(oml / omm) * opz ** (-1.5)
+    dxdz = math.sqrt(oml / omm) * opz ** (-2.5) * (-1.5)
     const1 = 2 * math.sqrt(1 + omm / oml) / (3.0 * HUBBLE * p.Hubble_h)
     numer = dxdz * (1 + x * (x * x + 1) ** -0.5)
     denom = x + math.sqrt(x * x + 1)
