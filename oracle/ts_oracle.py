@@ -665,10 +665,11 @@ def alpha_A(T):
 def get_Ts(cm: Cosmo, T: TsTables, z, delta, TK, xe, Jalpha):
     """get_Ts(float z, float delta, float TK, float xe, float Jalpha) vectorised; returns (TS, xalpha) float32."""
     zd = float(f32(z))
-    delta = np.asarray(delta, f32).astype(np.float64)
-    TKd = np.asarray(TK, f32).astype(np.float64)
-    xe = np.asarray(xe, f32).astype(np.float64)
-    Ja = np.asarray(Jalpha, f32).astype(np.float64)
+    shape = np.shape(TK)
+    delta = np.asarray(delta, f32).astype(np.float64).ravel()
+    TKd = np.asarray(TK, f32).astype(np.float64).ravel()
+    xe = np.asarray(xe, f32).astype(np.float64).ravel()
+    Ja = np.asarray(Jalpha, f32).astype(np.float64).ravel()
     Trad = TCMB * (1.0 + zd)
     opz3 = (1.0 + zd) ** 3.0
     nH = (1.0 - xe) * cm.No * opz3 * (1.0 + delta)
@@ -702,7 +703,7 @@ def get_Ts(cm: Cosmo, T: TsTables, z, delta, TK, xe, Jalpha):
     coll = ~wf
     TS[coll] = 1.0 / ((1.0 / Trad + xc[coll] / TKd[coll]) / (1.0 + xc[coll]))
     TS = np.where(TS < 0.0, np.abs(TS), TS)
-    return TS.astype(f32), xa.astype(f32)
+    return TS.astype(f32).reshape(shape), xa.astype(f32).reshape(shape)
 
 
 def dT_comp(cm: Cosmo, z, TK, xe):
