@@ -210,6 +210,23 @@ int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int m
 int rg_debug_ts_tables(const rg_params* p, const rg_snapshot* s, int n_hist, double x_e_ave,
                        double collapse_fraction, int max_shells, double* shells, double* freq, float* coef);
 
+/* ---- allocation-free round trip (no counterpart in the reference) ----
+   rg_debug_filter_roundtrip without a context and without any device allocation, for
+   callers that cannot allocate: one that has given the device's memory to its own pool,
+   or one for which cudaMalloc's implicit synchronisation is too costly.  Working memory is
+   a static device array of RG_NOALLOC_SCRATCH_BYTES bytes per device, which holds grids up
+   to RG_NOALLOC_MAX_GRID_DIM; larger ReionGridDim values return RG_EUNSUPPORTED with the
+   reason in errbuf.  Runs on the current device, on `stream` (a cudaStream_t; NULL = the
+   default stream), asynchronously.  The first call on a device looks up the array's address
+   (once per device); make it before any stream capture begins.  Nothing in the scratch has
+   to start at zero.  Two calls in flight at once on one device race on the scratch: order
+   them (one stream, or the caller's own synchronisation).  errbuf (may be NULL) receives
+   a message when the status is not RG_OK. */
+#define RG_NOALLOC_MAX_GRID_DIM 64
+#define RG_NOALLOC_SCRATCH_BYTES 2163200   /* 2 x (33 x 64 x 64) complex spectra + 64 twiddles */
+int rg_filter_roundtrip_noalloc(const rg_params* p, const float* d_in_padded, float* d_out_padded, double R,
+                                int filter_type, void* stream, char* errbuf, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

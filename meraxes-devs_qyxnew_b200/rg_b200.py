@@ -116,6 +116,8 @@ _SIGS = {
     "rg_radius_schedule": (C.c_int, [_P(rg_params), C.c_double, _P(C.c_double), C.c_int, _P(C.c_int)]),
     "rg_debug_ts_tables": (C.c_int, [_P(rg_params), _P(rg_snapshot), C.c_int, C.c_double, C.c_double, C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rg_filter_roundtrip_noalloc": (C.c_int, [_P(rg_params), C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                              C.c_void_p, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None
