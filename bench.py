@@ -2,19 +2,23 @@
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME] [--mode fused|plain]
 
-One step = one snapshot of the configured workload on seeded synthetic grids
-(inputs resident in HBM before the timed region).  The metric is ms per
-snapshot (lower is better), whole-job: with N ranks each rank processes its own
-snapshot per step (independent replicas: a snapshot does not shard), so the job
-time per snapshot is the max-over-ranks step time divided by N.
+One step = one snapshot of the configured workload on seeded synthetic grids, with
+the inputs resident in HBM before the timed region.  The default workload is the
+full step at 512^3 (box 500 Mpc/h, z = 8): ComputeTs (40 shells) -> find_HII_bubbles
+(61 radii) -> delta_T, in the reference's order (src/core/dracarys.c:383-391).
+``--config c1_256`` times find_HII_bubbles alone at 256^3.
 
-Between timed steps the per-cell state is reset and a 512 MiB buffer is written
-to flush L2; each step is timed with CUDA events on the stream the library
-launches on.  ``e2e`` times the host-buffer entry point (pinned host inputs,
-host<->device copies inside the timed region).  ``roofline`` comes from a
-separate pass with the library's per-kernel CUDA-event timing switched on.
-``--impl reference`` times the CPU restatement of the reference algorithm
-(the reference itself cannot be built: FFTW/GSL/HDF5/MPI are absent).
+The metric is ms per snapshot (lower is better), whole job: with N ranks each rank
+processes its own snapshot per step (independent replicas: a snapshot does not
+shard), so the job time per snapshot is the max-over-ranks step time divided by N.
+
+Between timed steps the per-cell state is restored and a 512 MiB buffer is written
+to flush L2; each step is timed with CUDA events on the stream the library launches
+on.  ``e2e`` times the host-buffer entry points (pinned host inputs, host<->device
+copies inside the timed region).  ``roofline`` comes from a separate pass with the
+library's per-kernel CUDA-event timing switched on.  ``--impl reference`` times the
+CPU restatement of the reference algorithm on bounded samples (the reference itself
+cannot be built: FFTW/GSL/HDF5/MPI are absent).
 """
 
 from __future__ import annotations
@@ -40,6 +44,7 @@ import numpy as np  # noqa: E402
 import workloads as wl  # noqa: E402
 
 METRIC = "ms/snapshot find_HII_bubbles+Ts at 256^3/512^3"
+DEFAULT_CONFIG = "c4_512"
 
 
 def parse():
@@ -48,7 +53,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1_256")
+    ap.add_argument("--config", default=DEFAULT_CONFIG)
     ap.add_argument("--mode", default="fused", choices=["fused", "plain"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -66,14 +71,40 @@ def config_params(cfg: wl.GridConfig, rg):
     return rg.make_params(cfg.n, cfg.box, Flag_EvolvingReionRBubbleMax=cfg.evolving_rmax,
                           ReionRBubbleMax=cfg.r_bubble_max, ReionRBubbleMin=cfg.r_bubble_min,
                           ReionDeltaRFactor=cfg.delta_r_factor, ReionFilterType=cfg.filter_type,
-                          ReionEfficiency=cfg.efficiency, ReionUVBFlag=cfg.uvb_flag)
+                          ReionEfficiency=cfg.efficiency, ReionUVBFlag=cfg.uvb_flag,
+                          Flag_IncludeSpinTemp=cfg.spin_temp, TsHeatingFilterType=cfg.ts_filter_type,
+                          TsNumFilterSteps=cfg.ts_steps)
+
+
+def oracle_params(cfg: wl.GridConfig):
+    import reion_oracle as ro
+    return ro.Params(ReionGridDim=cfg.n, BoxSize=cfg.box, Flag_EvolvingReionRBubbleMax=cfg.evolving_rmax,
+                     ReionRBubbleMax=cfg.r_bubble_max, ReionRBubbleMin=cfg.r_bubble_min,
+                     ReionDeltaRFactor=cfg.delta_r_factor, ReionFilterType=cfg.filter_type,
+                     ReionEfficiency=cfg.efficiency, ReionUVBFlag=cfg.uvb_flag, Flag_IncludeSpinTemp=cfg.spin_temp,
+                     TsHeatingFilterType=cfg.ts_filter_type, TsNumFilterSteps=cfg.ts_steps)
 
 
 def workload_desc(cfg: wl.GridConfig, nr: int) -> dict:
-    return {"workload": f"find_HII_bubbles {cfg.n}^3 float32, box {cfg.box:g} Mpc/h, z={cfg.z:g}, "
-                        f"filter {cfg.filter_type}, {nr} radii, ReionEfficiency {cfg.efficiency:g}",
-            "grid": cfg.n, "box_mpc_h": cfg.box, "redshift": cfg.z, "radii": nr,
-            "filter_type": cfg.filter_type, "l2": "flushed (512 MiB write) before every timed step; inputs > L2"}
+    what = "ComputeTs -> find_HII_bubbles -> delta_T" if cfg.spin_temp else "find_HII_bubbles"
+    ts = f", {cfg.ts_steps} Ts shells (heating filter {cfg.ts_filter_type})" if cfg.spin_temp else ""
+    return {"workload": f"{what}, {cfg.n}^3 float32, box {cfg.box:g} Mpc/h, z={cfg.z:g}, "
+                        f"filter {cfg.filter_type}, {nr} radii{ts}, ReionEfficiency {cfg.efficiency:g}",
+            "name": cfg.name, "grid": cfg.n, "box_mpc_h": cfg.box, "redshift": cfg.z, "radii": nr,
+            "ts_shells": cfg.ts_steps if cfg.spin_temp else 0, "filter_type": cfg.filter_type,
+            "l2": "flushed (512 MiB write) before every timed step; inputs > L2"}
+
+
+def alg_bytes(cfg: wl.GridConfig, nr: int, live_grids: int) -> float:
+    """Algorithmic HBM bytes per snapshot (B_HII + B_Ts + B_dT), Nc = N^2 (N/2 + 1)."""
+    n = cfg.n
+    n3 = float(n) ** 3
+    nc = float(n) * n * (n // 2 + 1)
+    b = live_grids * (4 * n3 + 8 * nc) + nr * (live_grids * 8 * nc + 8 * n3) + 24 * n3
+    if cfg.spin_temp:
+        b += cfg.ts_steps * (2 * (4 * n3 + 16 * nc) + 36 * n3) + 24 * n3
+        b += 16 * n3
+    return b
 
 
 class ClockSampler:
@@ -146,53 +177,283 @@ def traffic_from_profiles(kernel: str, cfg_name: str):
 
 
 # ---------------------------------------------------------------------------
+# inputs
 
-def cpu_sample(cfg: wl.GridConfig, src, sample_radii: int = 4):
-    """Time the CPU restatement (oracle, float32 pocketfft on all cores) on a bounded
-    sample of one snapshot: the forward transforms, ``sample_radii`` filter radii and
-    the closing pass, extrapolated to the full radius count."""
+def history_slots(cfg, rg, zz, snap):
+    """History slots the shells use (from the library's host coefficient engine, no device work)."""
+    p = config_params(cfg, rg)
+    _, _, coef = rg.ts_tables(p, zz, snap, snap + 1, 2e-4, 1e-3, np.zeros(len(zz)), with_freq=False)
+    used = np.nonzero(np.any(coef != 0, axis=0))[0]
+    return int(used.max()) if used.size else 0       # sources 1..k = history slots 0..k-1
+
+
+def make_inputs(cfg, rank, zz, snap, n_hist):
+    src = wl.make_sources(cfg.n, cfg.box, cfg.seed + rank, cfg.source_scale)
+    ti = wl.make_config_ts_inputs(src, zz, snap, n_hist) if cfg.spin_temp else None
+    return src, ti
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement on bounded samples
+
+def cpu_sample(cfg, src, ti, zz, snap, radii: int = 1, shells: int = 1, table_shells: int = 2,
+               cell_planes: int = 0):
+    """Time the oracle (float32 pocketfft on all host cores) on a bounded sample of one
+    snapshot and extrapolate to the whole snapshot:
+      find_HII_bubbles: forward r2c of every grid, ``radii`` of the nR radii, closing pass;
+      ComputeTs: ``shells`` of the nS shells (FFTs, filter, sums), the frequency tables of
+      ``table_shells`` shells, and the per-cell update on ``cell_planes`` x-planes;
+      delta_T in full.  Returns (ms per snapshot, description, wall seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import reion_oracle as ro
     import tables
     ro.set_recfast(tables.Recfast(tables.default_tables_dir()).T)
-    p = ro.Params(ReionGridDim=cfg.n, BoxSize=cfg.box, Flag_EvolvingReionRBubbleMax=cfg.evolving_rmax,
-                  ReionRBubbleMax=cfg.r_bubble_max, ReionRBubbleMin=cfg.r_bubble_min,
-                  ReionDeltaRFactor=cfg.delta_r_factor, ReionFilterType=cfg.filter_type,
-                  ReionEfficiency=cfg.efficiency, ReionUVBFlag=cfg.uvb_flag)
-    st = ro.HIIState.fresh(cfg.n)
-    t0 = time.perf_counter()
+    p = oracle_params(cfg)
+    n = cfg.n
+    U = wl.from_padded
+    wall0 = time.perf_counter()
+    st = ro.HIIState.fresh(n)
+    xe = U(ti.x_e_box_prev) if ti is not None else None
+    tk = ti.Tk_box if ti is not None else None
     _, _, _, diag = ro.find_hii_bubbles(p, cfg.z, src.deltax, src.stars, src.sfr, st, "fp32",
-                                        radius_subset=sample_radii, with_dead_grids=True)
-    wall = time.perf_counter() - t0
+                                        x_e_box=xe, Tk_box=tk, radius_subset=radii, with_dead_grids=True)
     nr = diag["n_radii"]
     t = diag["timing"]
     est = t["forward"] + t["per_radius"] * nr + t["final"]
-    return est * 1e3, wall, nr, os.cpu_count()
+    desc = f"find_HII_bubbles: forward r2c + {radii} of {nr} radii + closing pass, extrapolated to {nr} radii"
+    if ti is not None:
+        import ts_oracle as to
+        T = to.TsTables()
+        to.gk61_rule()                 # the quadrature rule is set up once, outside the timed parts
+        cm = to.Cosmo(p)
+        zp = float(zz[snap])
+        nS = p.TsNumFilterSteps
+        planes = cell_planes or max(1, n // 64)
+        xprev = U(ti.x_e_box_prev)
+        # history re-weighting of the source grids (elementwise): timed on `planes` x-planes
+        t0 = time.perf_counter()
+        sh, _ = to.shells_and_sources(p, zz, snap, U(src.sfr)[:planes], U(src.xray)[:planes],
+                                      [U(a)[:planes] for a in ti.sfr_histories],
+                                      [U(a)[:planes] for a in ti.xray_histories])
+        t_setup = (time.perf_counter() - t0) * n / planes
+        # frequency tables of table_shells shells
+        sub = to.Shells()
+        for k in ("R", "zpp_edge", "zpp", "dzpp", "dt_dzpp"):
+            setattr(sub, k, getattr(sh, k)[:table_shells])
+        sub.final_weight = sh.final_weight
+        t0 = time.perf_counter()
+        heat, ion, lya, sum_lyn = to.freq_tables(p, T, sub, zp, float(np.mean(xprev)), 1e-3, zz, ti.stored_fcoll,
+                                                 snap)
+        t_tab = (time.perf_counter() - t0) * nS / table_shells
+        tabs = tuple(np.repeat(a[:, :1], nS, axis=1) for a in (heat, ion, lya))
+        lyn = np.repeat(sum_lyn[:1], nS)
+        # x_e interpolation nodes (once per snapshot), then `shells` filtered shells in full
+        t0 = time.perf_counter()
+        xi = to.xe_interp_index(T, xprev)
+        sums = [np.zeros(xprev.shape) for _ in range(4)]
+        t_xi = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for r in range(shells):
+            to.shell_accumulate(p, sh, r + 1, U(src.sfr), U(src.xray), xi, tabs, lyn, zp, sums, "fp32")
+        t_shell = (time.perf_counter() - t0) / shells * nS
+        # the per-cell update on `planes` x-planes
+        pf = to.prefactors(p, zp)
+        d = U(src.deltax)[:planes]
+        part = [a[:planes] for a in sums]
+        t0 = time.perf_counter()
+        to.finish_sums(p, cm, pf, zp, d, part)
+        to.evolve_cells(p, cm, T, pf, zp, zp - float(zz[snap - 1]), d, xprev[:planes], ti.Tk_box[:planes], part)
+        t_cell = (time.perf_counter() - t0) * n / planes
+        del sums, xi
+        est += t_setup + t_tab + t_xi + t_shell + t_cell
+        desc += (f"; ComputeTs: history re-weighting on {planes} of {n} planes x {n / planes:g}, frequency "
+                 f"tables of {table_shells} shells x {nS / table_shells:g}, {shells} of {nS} shells "
+                 f"(r2c, filter, c2r, sums) x {nS}, per-cell update on {planes} of {n} planes x {n / planes:g}")
+        t0 = time.perf_counter()
+        ro.delta_T(p, cfg.z, np.full((n, n, n), 0.5, np.float32), U(src.deltax), ti.Tk_box)
+        est += time.perf_counter() - t0
+        desc += "; delta_T in full"
+    return est * 1e3, desc, time.perf_counter() - wall0, nr
 
 
 def run_reference(args, cfg):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    src = wl.make_sources(cfg.n, cfg.box, cfg.seed, cfg.source_scale)
+    zz, snap = wl.snapshot_redshifts(cfg.z)
+    n_hist = snap + 1 if cfg.spin_temp else 0
+    if cfg.spin_temp:
+        import rg_b200 as rg
+        n_hist = history_slots(cfg, rg, zz, snap)
+    src, ti = make_inputs(cfg, 0, zz, snap, n_hist)
     vals = []
-    nr = 0
+    nr, desc = 0, ""
     for i in range(args.warmup + args.steps):
-        ms, wall, nr, cores = cpu_sample(cfg, src)
+        ms, desc, wall, nr = cpu_sample(cfg, src, ti, zz, snap)
         if i >= args.warmup:
             vals.append(ms)
     v = statistics.mean(vals)
-    sample = (f"1 snapshot of {cfg.n}^3: forward r2c + 4 of {nr} radii + closing pass per step, "
-              f"extrapolated to {nr} radii")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/snapshot", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
             "config": workload_desc(cfg, nr),
             "cpu_baseline": {"value": v, "unit": "ms/snapshot", "cores": os.cpu_count(), "kind": "port",
-                             "sample": sample + "; oracle restatement, scipy pocketfft float32, all host cores "
-                                                "(the reference needs FFTW/GSL/MPI, absent here)"},
+                             "sample": desc + "; oracle restatement, scipy pocketfft float32, all host cores "
+                                              "(the reference needs FFTW/GSL/MPI, absent here)"},
             "e2e": {"value": v, "unit": "ms/snapshot", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+
+class Workload:
+    """Device grids of one snapshot and the step through the library's device entry points."""
+
+    def __init__(self, cfg, rg, torch, dev, ctx, src, ti, zz, snap, n_hist):
+        self.cfg, self.rg, self.torch, self.dev, self.ctx = cfg, rg, torch, dev, ctx
+        n = cfg.n
+        self.n = n
+        npad = n * n * 2 * (n // 2 + 1)
+        nreal = n ** 3
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32).ravel()).to(dev)
+        b = {"deltax": t(src.deltax), "stars": t(src.stars), "weighted_sfr": t(src.sfr)}
+        for k in ("xH", "r_bubble", "z_at_ionization", "J_21_at_ionization", "temp_kinetic_all_gas", "delta_T"):
+            b[k] = torch.zeros(nreal, device=dev)
+        self.spin = bool(cfg.spin_temp)
+        if self.spin:
+            b["sfr"] = t(src.sfr)
+            b["xray_luminosity"] = t(src.xray)
+            b["x_e_box_prev"] = t(ti.x_e_box_prev)
+            b["x_e_box"] = torch.zeros(npad, device=dev)
+            b["Tk_box"] = t(ti.Tk_box)
+            b["TS_box"] = torch.zeros(nreal, device=dev)
+            self.xe0 = b["x_e_box_prev"].clone()
+            self.tk0 = b["Tk_box"].clone()
+            if n_hist:
+                b["sfr_histories"] = torch.cat([t(a) for a in ti.sfr_histories])
+                b["xray_luminosity_histories"] = torch.cat([t(a) for a in ti.xray_histories])
+        self.b = b
+        g = rg.rg_grids()
+        for k, v in b.items():
+            setattr(g, k, v.data_ptr())
+        g.n_hist = n_hist
+        self.g = g
+        self.p = config_params(cfg, rg)
+        self.sf0 = ti.stored_fcoll.copy() if ti is not None else np.zeros(len(zz))
+        self.sf = self.sf0.copy()
+        self.s = rg.snapshot(zz, snap, self.sf)
+        self.hii = rg.rg_hii_scalars()
+        self.ts = rg.rg_ts_scalars()
+        self.tb = C.c_double()
+        self.flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def reset(self):
+        b = self.b
+        b["z_at_ionization"].fill_(-1.0)
+        b["J_21_at_ionization"].zero_()
+        b["temp_kinetic_all_gas"].zero_()
+        if self.spin:
+            b["x_e_box_prev"].copy_(self.xe0)
+            b["Tk_box"].copy_(self.tk0)
+        self.sf[:] = self.sf0
+        self.flush.zero_()
+
+    def step(self):
+        ctx, g, p, s = self.ctx, C.byref(self.g), C.byref(self.p), C.byref(self.s)
+        if self.spin:
+            ctx.call("rg_compute_Ts", p, s, g, C.byref(self.ts))
+        ctx.call("rg_find_HII_bubbles", p, s, g, C.byref(self.hii))
+        if self.spin:
+            ctx.call("rg_delta_T", p, s, g, C.byref(self.tb))
+
+
+class HostWorkload:
+    """The same snapshot through the host-buffer entry points (pinned host arrays)."""
+
+    def __init__(self, wk: Workload, src, ti, n_hist):
+        torch, rg = wk.torch, wk.rg
+        self.wk = wk
+        n = wk.n
+        nreal = n ** 3
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32).ravel()).pin_memory()
+        h = {"deltax": pin(src.deltax), "stars": pin(src.stars), "weighted_sfr": pin(src.sfr)}
+        for k in ("xH", "r_bubble", "J_21_at_ionization", "temp_kinetic_all_gas", "delta_T"):
+            h[k] = torch.zeros(nreal).pin_memory()
+        h["z_at_ionization"] = torch.full((nreal,), -1.0).pin_memory()
+        if wk.spin:
+            h["sfr"] = pin(src.sfr)
+            h["xray_luminosity"] = pin(src.xray)
+            h["x_e_box_prev"] = pin(ti.x_e_box_prev)
+            h["x_e_box"] = torch.zeros_like(h["x_e_box_prev"]).pin_memory()
+            h["Tk_box"] = pin(ti.Tk_box)
+            h["TS_box"] = torch.zeros(nreal).pin_memory()
+            self.xe0 = h["x_e_box_prev"].clone()
+            self.tk0 = h["Tk_box"].clone()
+            if n_hist:
+                h["sfr_histories"] = torch.cat([pin(a) for a in ti.sfr_histories]).pin_memory()
+                h["xray_luminosity_histories"] = torch.cat([pin(a) for a in ti.xray_histories]).pin_memory()
+        self.h = h
+        hg = rg.rg_grids()
+        for k, v in h.items():
+            setattr(hg, k, v.data_ptr())
+        hg.n_hist = n_hist
+        self.hg = hg
+        bp = 4 * n * n * 2 * (n // 2 + 1)
+        br = 4 * nreal
+        # bytes each entry point copies (rg_api.cu / rg_dT.cu / rg_ts.cu host forms)
+        h2d = 3 * bp + 3 * br                                   # find_HII: deltax, stars, weighted_sfr, 3 state
+        d2h = 5 * br
+        if wk.spin:
+            h2d += bp + br                                      # find_HII: x_e_box, Tk_box
+            used = history_slots(wk.cfg, rg, *self.zzsnap()) + 1   # source grids staged by rg_compute_Ts_host
+            h2d += 3 * bp + br + 2 * used * bp                  # Ts: deltax, stars, x_e_box_prev, Tk_box, sources
+            d2h += 2 * bp + 2 * br                              # Ts: x_e_box_prev, x_e_box, Tk_box, TS_box
+            h2d += bp + 2 * br                                  # delta_T: deltax, xH, TS_box
+            d2h += br                                           # delta_T: delta_T
+        self.h2d, self.d2h = h2d, d2h
+
+    def zzsnap(self):
+        s = self.wk.s
+        return np.ctypeslib.as_array(s.ZZ, shape=(s.n_snapshots,)).copy(), s.snapshot
+
+    def reset(self):
+        h = self.h
+        h["z_at_ionization"].fill_(-1.0)
+        h["J_21_at_ionization"].zero_()
+        h["temp_kinetic_all_gas"].zero_()
+        if self.wk.spin:
+            h["x_e_box_prev"].copy_(self.xe0)
+            h["Tk_box"].copy_(self.tk0)
+        self.wk.sf[:] = self.wk.sf0
+        self.wk.flush.zero_()
+
+    def step(self):
+        wk = self.wk
+        ctx, g, p, s = wk.ctx, C.byref(self.hg), C.byref(wk.p), C.byref(wk.s)
+        if wk.spin:
+            ctx.call("rg_compute_Ts_host", p, s, g, C.byref(wk.ts))
+        ctx.call("rg_find_HII_bubbles_host", p, s, g, C.byref(wk.hii))
+        if wk.spin:
+            ctx.call("rg_delta_T_host", p, s, g, C.byref(wk.tb))
+
+
+def timed(torch, stream, fn, reset, warmup, steps):
+    for _ in range(warmup):
+        reset()
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
 
 
 def run_ours(args, cfg):
@@ -201,59 +462,30 @@ def run_ours(args, cfg):
 
     ws, rank, local = dist_env()
     if ws > 1:
+        import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    n = cfg.n
-    src = wl.make_sources(n, cfg.box, cfg.seed + rank, cfg.source_scale)
-    p = config_params(cfg, rg)
     zz, snap = wl.snapshot_redshifts(cfg.z)
-    s = rg.snapshot(zz, snap)
-    ctx = rg.Context(n, device=local)
+    n_hist = history_slots(cfg, rg, zz, snap) if cfg.spin_temp else 0
+    src, ti = make_inputs(cfg, rank, zz, snap, n_hist)
+    ctx = rg.Context(cfg.n, device=local)
     ctx.call("rg_set_mode", rg.RG_MODE_PLAIN if args.mode == "plain" else rg.RG_MODE_FUSED)
     stream = torch.cuda.current_stream(dev)
     ctx.call("rg_set_stream", C.c_void_p(stream.cuda_stream))
-
-    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32).ravel()).to(dev)
-    nreal = n ** 3
-    bufs = {"deltax": t(src.deltax), "stars": t(src.stars), "weighted_sfr": t(src.sfr)}
-    for k in ("xH", "r_bubble", "z_at_ionization", "J_21_at_ionization", "temp_kinetic_all_gas"):
-        bufs[k] = torch.zeros(nreal, device=dev)
-    g = rg.rg_grids()
-    for k, v in bufs.items():
-        setattr(g, k, v.data_ptr())
-    out = rg.rg_hii_scalars()
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
-    def reset():
-        bufs["z_at_ionization"].fill_(-1.0)
-        bufs["J_21_at_ionization"].zero_()
-        bufs["temp_kinetic_all_gas"].zero_()
-        flush.zero_()
-
-    def step():
-        ctx.call("rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(g), C.byref(out))
+    wk = Workload(cfg, rg, torch, dev, ctx, src, ti, zz, snap, n_hist)
 
     for _ in range(args.warmup):
-        reset()
-        step()
+        wk.reset()
+        wk.step()
     torch.cuda.synchronize(dev)
     if ws > 1:
         torch.distributed.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    times = []
-    for _ in range(args.steps):
-        reset()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+    times = timed(torch, stream, wk.step, wk.reset, 0, args.steps)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
     ms_step = statistics.mean(times)
@@ -262,82 +494,65 @@ def run_ours(args, cfg):
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         ms_step = float(tt.item())
         torch.distributed.barrier()
-    nr = out.n_radii
+    nr = wk.hii.n_radii
     value = ms_step / ws
+    results = {"mean_xH": wk.hii.volume_weighted_global_xH}
+    if wk.spin:
+        results.update(mean_TS=wk.ts.volume_ave_TS, mean_TK=wk.ts.volume_ave_TK, mean_xe=wk.ts.volume_ave_xe,
+                       mean_Tb=wk.tb.value, collapse_fraction=wk.ts.collapse_fraction)
 
-    # e2e through the host-buffer entry point: pinned host inputs and outputs
+    # e2e through the host-buffer entry points
     e2e = None
     if not args.no_e2e:
-        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32).ravel()).pin_memory()
-        hb = {"deltax": pin(src.deltax), "stars": pin(src.stars), "weighted_sfr": pin(src.sfr)}
-        for k in ("xH", "r_bubble", "J_21_at_ionization", "temp_kinetic_all_gas"):
-            hb[k] = torch.zeros(nreal).pin_memory()
-        hb["z_at_ionization"] = torch.full((nreal,), -1.0).pin_memory()
-        hg = rg.rg_grids()
-        for k, v in hb.items():
-            setattr(hg, k, v.data_ptr())
-        h2d = sum(hb[k].numel() * 4 for k in ("deltax", "stars", "weighted_sfr", "z_at_ionization",
-                                              "J_21_at_ionization", "temp_kinetic_all_gas"))
-        d2h = sum(hb[k].numel() * 4 for k in ("xH", "r_bubble", "z_at_ionization", "J_21_at_ionization",
-                                              "temp_kinetic_all_gas"))
-        o2 = rg.rg_hii_scalars()
-        et = []
-        for i in range(args.warmup + args.steps):
-            hb["z_at_ionization"].fill_(-1.0)
-            hb["J_21_at_ionization"].zero_()
-            hb["temp_kinetic_all_gas"].zero_()
-            flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            ctx.call("rg_find_HII_bubbles_host", C.byref(p), C.byref(s), C.byref(hg), C.byref(o2))
-            e1.record(stream)
-            e1.synchronize()
-            if i >= args.warmup:
-                et.append(e0.elapsed_time(e1))
+        hw = HostWorkload(wk, src, ti, n_hist)
+        et = timed(torch, stream, hw.step, hw.reset, args.warmup, args.steps)
         em = statistics.mean(et)
         if ws > 1:
             tt = torch.tensor([em], device=dev)
             torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
             em = float(tt.item())
-        e2e = {"value": em / ws, "unit": "ms/snapshot", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        e2e = {"value": em / ws, "unit": "ms/snapshot", "h2d_bytes_per_step": hw.h2d, "d2h_bytes_per_step": hw.d2h}
+        del hw
 
     # roofline pass: per-kernel CUDA events inside the library
+    nprof = max(2, min(args.steps, 3))
     ctx.profile(True)
-    for _ in range(max(2, min(args.steps, 3))):
-        reset()
-        step()
+    for _ in range(nprof):
+        wk.reset()
+        wk.step()
     stats = ctx.kernel_stats()
     ctx.profile(False)
-    launches = sum(k["launches"] for k in stats) // max(2, min(args.steps, 3))
+    launches = sum(k["launches"] for k in stats) // nprof
     top = max(stats, key=lambda k: k["ms_total"])
     peak, peak_kind = measured_peak()
     ach = top["alg_bytes_total"] / (top["ms_total"] * 1e-3) / 1e9
     per_launch_bytes = top["alg_bytes_total"] / top["launches"]
     traffic = traffic_from_profiles(top["name"], cfg.name)
     total_ms = sum(k["ms_total"] for k in stats)
+    live = 3 if cfg.spin_temp else 2       # filtered grids in fused mode: deltax, stars (+ x_e)
+    step_bytes = alg_bytes(cfg, nr, live + (1 if args.mode == "plain" else 0))
     roofline = {"bound": "hbm", "kernel": top["name"], "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "alg_bytes_per_launch": per_launch_bytes,
                 "share_of_step": top["ms_total"] / total_ms if total_ms > 0 else None,
-                "kernels": {k["name"]: {"launches": k["launches"], "ms": k["ms_total"],
+                "step_alg_bytes": step_bytes, "step_GBps": step_bytes / (ms_step * 1e-3) / 1e9,
+                "step_frac": step_bytes / (ms_step * 1e-3) / 1e9 / peak,
+                "kernels": {k["name"]: {"launches": k["launches"] // nprof, "ms": k["ms_total"] / nprof,
                                         "GBps": k["alg_bytes_total"] / max(k["ms_total"], 1e-9) / 1e6}
                             for k in stats}}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        ms_cpu, wall, nr_c, cores = cpu_sample(cfg, src)
-        cpu = {"value": ms_cpu, "unit": "ms/snapshot", "cores": cores, "kind": "port",
-               "sample": f"1 snapshot of {n}^3: forward r2c + 4 of {nr_c} radii + closing pass, extrapolated to "
-                         f"{nr_c} radii; oracle restatement, scipy pocketfft float32 on all host cores "
-                         f"({wall:.1f} s wall)"}
+        ms_cpu, desc, wall, _ = cpu_sample(cfg, src, ti, zz, snap)
+        cpu = {"value": ms_cpu, "unit": "ms/snapshot", "cores": os.cpu_count(), "kind": "port",
+               "sample": desc + f"; oracle restatement, scipy pocketfft float32 on all host cores ({wall:.1f} s wall)"}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "ms/snapshot", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, BASELINE shapes)",
                 "config": dict(workload_desc(cfg, nr), mode=args.mode, parallelism=f"replicas x{ws}"),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clk, "mean_xH": out.volume_weighted_global_xH}
+                "clocks": clk, "results": results}
         print(json.dumps(line), flush=True)
     ctx.close()
     if ws > 1:

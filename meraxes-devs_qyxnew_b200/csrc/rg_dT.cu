@@ -50,7 +50,10 @@ __global__ void __launch_bounds__(DT_NT) k_delta_T(const float* __restrict__ xH,
 int delta_T_launch(rg_context* ctx, int n, const float* xH, const float* deltax, const float* TS, float* dT,
                    float const_factor, double t_rad, int spin, int pec_gt1, float redshift, double* partials,
                    int nblocks, cudaStream_t st) {
+  prof_begin(ctx, "delta_T", st);
   k_delta_T<<<nblocks, DT_NT, 0, st>>>(xH, deltax, TS, dT, n, const_factor, t_rad, spin, pec_gt1, redshift, partials);
+  // xH, deltax (and TS) read, delta_T written
+  prof_end(ctx, (double)n * n * n * (spin ? 16.0 : 12.0), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }

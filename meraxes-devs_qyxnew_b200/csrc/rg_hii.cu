@@ -544,13 +544,17 @@ int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int
                  cudaStream_t st) {
   const double delta_k = 2.0 * M_PI / box;
   const int bx = (n2max + 1 + 255) / 256;
+  prof_begin(ctx, "window_table", st);
   k_window_table<<<dim3(bx < 1024 ? bx : 1024, nr), 256, 0, st>>>(d_wtab, n2max, d_radii, nr, delta_k, ftype);
+  prof_end(ctx, 4.0 * (n2max + 1) * nr, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 
 int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out, cudaStream_t st) {
+  prof_begin(ctx, "reduce_partials", st);
   k_reduce_partials<<<1, 256, 0, st>>>(partials, nblocks, nsum, d_out);
+  prof_end(ctx, 8.0 * nblocks * nsum, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }

@@ -661,7 +661,9 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   };
 
   // collapse fraction and <x_e> (both branches compute the collapse fraction)
+  prof_begin(ctx, "ts_reduce0", st);
   k_ts_reduce0<<<nblk, 256, 0, st>>>(g->stars, g->deltax, g->x_e_box_prev, N, Mh2, ftpr3, partials);
+  prof_end(ctx, 12.0 * n3, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   if ((rc = reduce_partials(ctx, partials, nblk, 2, ctx->d_sums, st))) return rc;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
@@ -674,8 +676,10 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   if ((zp - p->ReionMaxHeatingRedshift) >= -0.0001) {
     const float xe0 = (float)xion_RECFAST(ctx->tables, (float)zp);
     const float TK0 = (float)T_RECFAST(ctx->tables, (float)zp);
+    prof_begin(ctx, "ts_homog", st);
     k_ts_homog<<<nblk, 256, 0, st>>>(d_hc, (float)zp, xe0, TK0, cT_approx((float)zp), N, g->deltax, g->x_e_box_prev,
                                       g->x_e_box, g->Tk_box, g->TS_box, partials, d_nonconv);
+    prof_end(ctx, 28.0 * n3, st);
     RG_CUDA_TRY(ctx, cudaGetLastError());
     return finish(true);
   }

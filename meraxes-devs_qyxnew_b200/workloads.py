@@ -165,6 +165,28 @@ class TsInputs:
     stored_fcoll: np.ndarray           # float64 [n_snapshots]
 
 
+def history_scale(zz: np.ndarray, snap: int, h: int) -> float:
+    """SFR history amplitude of slot h relative to this snapshot: ((1 + z_h) / (1 + z))^-3."""
+    zh = zz[snap - h] if snap - h >= 0 else zz[0]
+    return ((1.0 + zh) / (1.0 + zz[snap])) ** -3.0
+
+
+def make_config_ts_inputs(src: SourceGrids, zz: np.ndarray, snap: int, n_hist: int,
+                          fcoll_prev: float = 1e-5) -> TsInputs:
+    """The ComputeTs workload's state: uniform T_K = 12 K and x_e = 2e-4, and per-slot
+    SFR / X-ray histories = this snapshot's grids x ((1 + z_h) / (1 + z))^-3."""
+    n = src.n
+    xe = np.full(padded_shape(n), 2e-4, np.float32)
+    xe[:, :, n:] = 0.0
+    tk = np.full((n, n, n), 12.0, np.float32)
+    sfr_h = [(src.sfr * np.float32(history_scale(zz, snap, h))).astype(np.float32) for h in range(n_hist)]
+    xr_h = [(src.xray * np.float32(history_scale(zz, snap, h))).astype(np.float32) for h in range(n_hist)]
+    sf = np.zeros(len(zz))
+    if snap > 0:
+        sf[snap - 1] = fcoll_prev
+    return TsInputs(x_e_box_prev=xe, Tk_box=tk, sfr_histories=sfr_h, xray_histories=xr_h, stored_fcoll=sf)
+
+
 def make_ts_inputs(src: SourceGrids, zz: np.ndarray, snap: int, n_hist: int, seed: int,
                    fcoll_prev: float = 1e-5) -> TsInputs:
     """Synthetic ComputeTs state: x_e ~ 2e-4 LN(0, 0.3), T_K ~ 12 K (1 + 0.3 delta) floored at

@@ -726,7 +726,6 @@ def compute_ts(p: ro.Params, T: TsTables, ZZ, snapshot: int, stored_fcoll, g: di
     zp = float(ZZ[snapshot])
     box = p.BoxSize / p.Hubble_h
     pv = (box / float(n)) ** 3
-    u = ro.run_units(p)
     deltax = g["deltax"].astype(f32)
     stars = g["stars"].astype(f32)
     R0 = L_FACTOR * box / float(f32(n))
@@ -758,63 +757,102 @@ def compute_ts(p: ro.Params, T: TsTables, ZZ, snapshot: int, stored_fcoll, g: di
     prevz = zp if snapshot == 0 else float(ZZ[snapshot - 1])
     dzp = zp - prevz
     pf = prefactors(p, zp)
-    zpf = float(f32(zp))
-    n_b = cm.N_b0 * float(f32(1) + f32(zp)) ** 3 * (f32(1) + deltax).astype(np.float64)
-    dxheat = np.zeros(deltax.shape)
-    dxion = np.zeros(deltax.shape)
-    dxlya = np.zeros(deltax.shape)
-    dstar = np.zeros(deltax.shape)
+    sums = [np.zeros(deltax.shape) for _ in range(4)]
     if not no_light:
         sf = stored_fcoll if stored_fcoll is not None else np.zeros(len(ZZ))
         heat, ion, lya, sum_lyn = freq_tables(p, T, sh, zp, x_e_ave, collapse_fraction, ZZ, sf, snapshot)
         if tables_out is not None:
             tables_out.update(heat=heat, ion=ion, lya=lya, sum_lyn=sum_lyn, shells=sh)
-        # per-cell x_e interpolation index (ComputeTs.c:1198-1209)
-        X = T.X
-        xh = xprev.astype(np.float64)
-        xh = np.where(xh > float(X[-1]) * 0.999, float(X[-1]) * 0.999, np.where(xh < float(X[0]), 1.001 * float(X[0]), xh))
-        xhf = xh.astype(f32)
-        m_lo = np.full(xh.shape, len(X) - 1)
-        for m in range(len(X) - 1, -1, -1):
-            m_lo = np.where(xhf < X[m], m - 1, m_lo)
-        m_lo = np.clip(m_lo, 0, len(X) - 2)
-        Xl = X[m_lo].astype(np.float64)
-        Xh = X[m_lo + 1].astype(np.float64)
-        win_prec = "fp32" if precision == "fp32" else "fp64"
+        xi = xe_interp_index(T, xprev)
         for r in range(nS):
-            s_grid, x_grid = grids[r]
-            ss = ro.forward(s_grid, win_prec)
-            xs = ro.forward(x_grid, win_prec)
-            if r > 0:
-                w = ro.window(n, p.BoxSize, float(f32(sh.R[r])), p.TsHeatingFilterType, win_prec)
-                ss = ss * w
-                xs = xs * w
-            s_f = ro.inverse(ss, n)
-            x_f = ro.inverse(xs, n)
-            if precision == "fp32":
-                s_f = s_f.astype(f32)
-                x_f = x_f.astype(f32)
-            s_f = np.maximum(s_f, 0.0)
-            SFR = (s_f.astype(np.float64) / pv) * (p.UnitMass_in_g / u.UnitTime_in_s) * p.UnitLength_in_cm ** -3.0 / SOLAR_MASS
-            XR = (x_f.astype(np.float64) / pv) * XRAY_LUMINOSITY_UNIT * p.UnitLength_in_cm ** -3.0
+            shell_accumulate(p, sh, r, grids[r][0], grids[r][1], xi, (heat, ion, lya), sum_lyn, zp, sums, precision)
+        finish_sums(p, cm, pf, zp, deltax, sums)
+    res = evolve_cells(p, cm, T, pf, zp, dzp, deltax, xprev, g["Tk_box"], sums)
+    xn, tk, ts = res["x_e"], res["Tk"], res["TS"]
+    g["x_e_box_prev"][...] = xn
+    g["Tk_box"][...] = tk
+    g["TS_box"] = ts
+    g["x_e_box"] = xn.copy()
+    out.update(volume_ave_J_alpha=float(np.sum(res["J_alpha"]) / n3),
+               volume_ave_xalpha=float(np.sum(res["xalpha"].astype(np.float64)) / n3),
+               volume_ave_Xheat=float(np.sum(res["dxheat_dzp"]) / n3), volume_ave_Xion=float(np.sum(res["dxion"]) / n3),
+               volume_ave_TS=float(np.sum(ts.astype(np.float64)) / n3),
+               volume_ave_TK=float(np.sum(tk.astype(np.float64)) / n3),
+               volume_ave_xe=float(np.sum(xn.astype(np.float64)) / n3))
+    out["_cells"] = dict(dxheat_dzp=res["dxheat_dzp"], dxion=res["dxion"], J_alpha=res["J_alpha"])
+    return out
 
-            def fi(tbl):
-                lo = tbl[m_lo, r]
-                hi = tbl[m_lo + 1, r]
-                return (hi - lo) / (Xh - Xl) * (xh - Xl) + lo
 
-            zpp, dzpp, dt_dzpp = sh.zpp[r], sh.dzpp[r], sh.dt_dzpp[r]
-            integ = XR * (1 + zpp) ** (-p.SpecIndexXrayGal)
-            dxheat += dt_dzpp * dzpp * integ * fi(heat)
-            dxion += dt_dzpp * dzpp * integ * fi(ion)
-            dxlya += dt_dzpp * dzpp * integ * fi(lya)
-            dstar += SFR * float(f32(1) + f32(zp)) ** 2 * (1 + zpp) * sum_lyn[r] * dt_dzpp * dzpp
-        dxheat *= pf["const_zp"]
-        dxion *= pf["const_zp"]
-        dxlya *= pf["const_zp"] * n_b
-        dstar *= (SPEED_OF_LIGHT / (4.0 * math.pi)) / (PROTONMASS / SOLAR_MASS)
-    x_e = xprev.astype(np.float64)
-    Tk = g["Tk_box"].astype(f32)
+def xe_interp_index(T: TsTables, xprev):
+    """Per-cell x_e interpolation node and clamped x_e (ComputeTs.c:1198-1209)."""
+    X = T.X
+    xh = np.asarray(xprev, f32).astype(np.float64)
+    xh = np.where(xh > float(X[-1]) * 0.999, float(X[-1]) * 0.999, np.where(xh < float(X[0]), 1.001 * float(X[0]), xh))
+    xhf = xh.astype(f32)
+    m_lo = np.full(xh.shape, len(X) - 1)
+    for m in range(len(X) - 1, -1, -1):
+        m_lo = np.where(xhf < X[m], m - 1, m_lo)
+    m_lo = np.clip(m_lo, 0, len(X) - 2)
+    return dict(xh=xh, m_lo=m_lo, Xl=X[m_lo].astype(np.float64), Xh=X[m_lo + 1].astype(np.float64))
+
+
+def shell_accumulate(p: ro.Params, sh, r: int, s_grid, x_grid, xi: dict, tabs, sum_lyn, zp: float, sums: list,
+                     precision: str = "fp64"):
+    """One shell R_ct: FFT, filter (R_ct > 0), inverse, clamp and unit conversion of the sfr and
+    X-ray grids (ComputeTs.c:480-744), then its terms of the evolveInt sums
+    (XRayHeatingFunctions.c:1379-1432) added to sums = [heat, ion, lya, star]."""
+    n = p.ReionGridDim
+    box = p.BoxSize / p.Hubble_h
+    pv = (box / float(n)) ** 3
+    u = ro.run_units(p)
+    prec = "fp32" if precision == "fp32" else "fp64"
+    ss = ro.forward(s_grid, prec)
+    xs = ro.forward(x_grid, prec)
+    if r > 0:
+        w = ro.window(n, p.BoxSize, float(f32(sh.R[r])), p.TsHeatingFilterType, prec)
+        ss = ss * w
+        xs = xs * w
+    s_f = ro.inverse(ss, n)
+    x_f = ro.inverse(xs, n)
+    if precision == "fp32":
+        s_f = s_f.astype(f32)
+        x_f = x_f.astype(f32)
+    s_f = np.maximum(s_f, 0.0)
+    SFR = (s_f.astype(np.float64) / pv) * (p.UnitMass_in_g / u.UnitTime_in_s) * p.UnitLength_in_cm ** -3.0 / SOLAR_MASS
+    XR = (x_f.astype(np.float64) / pv) * XRAY_LUMINOSITY_UNIT * p.UnitLength_in_cm ** -3.0
+    m_lo, xh, Xl, Xh = xi["m_lo"], xi["xh"], xi["Xl"], xi["Xh"]
+
+    def fi(tbl):
+        lo = tbl[m_lo, r]
+        hi = tbl[m_lo + 1, r]
+        return (hi - lo) / (Xh - Xl) * (xh - Xl) + lo
+
+    zpp, dzpp, dt_dzpp = sh.zpp[r], sh.dzpp[r], sh.dt_dzpp[r]
+    integ = XR * (1 + zpp) ** (-p.SpecIndexXrayGal)
+    for k in range(3):
+        sums[k] += dt_dzpp * dzpp * integ * fi(tabs[k])
+    sums[3] += SFR * float(f32(1) + f32(zp)) ** 2 * (1 + zpp) * sum_lyn[r] * dt_dzpp * dzpp
+
+
+def finish_sums(p: ro.Params, cm: Cosmo, pf: dict, zp: float, deltax, sums: list):
+    """The prefactors evolveInt applies after its shell loop (XRayHeatingFunctions.c:1436-1447)."""
+    n_b = cm.N_b0 * float(f32(1) + f32(zp)) ** 3 * (f32(1) + np.asarray(deltax, f32)).astype(np.float64)
+    sums[0] *= pf["const_zp"]
+    sums[1] *= pf["const_zp"]
+    sums[2] *= pf["const_zp"] * n_b
+    sums[3] *= (SPEED_OF_LIGHT / (4.0 * math.pi)) / (PROTONMASS / SOLAR_MASS)
+
+
+def evolve_cells(p: ro.Params, cm: Cosmo, T: TsTables, pf: dict, zp: float, dzp: float, deltax, xprev, Tk_box,
+                 sums: list) -> dict:
+    """The rest of evolveInt, the Euler step of x_e and T_K and get_Ts, per cell
+    (XRayHeatingFunctions.c:1472-1561, ComputeTs.c:1371-1407); any subset of cells."""
+    dxheat, dxion, dxlya, dstar = sums
+    deltax = np.asarray(deltax, f32)
+    zpf = float(f32(zp))
+    n_b = cm.N_b0 * float(f32(1) + f32(zp)) ** 3 * (f32(1) + deltax).astype(np.float64)
+    x_e = np.asarray(xprev, f32).astype(np.float64)
+    Tk = np.asarray(Tk_box, f32)
     Td = Tk.astype(np.float64)
     sink = alpha_A(Td) * CLUMPING_FACTOR * x_e * x_e * cm.f_H * n_b
     dxe_dzp = pf["dt_dzp"] * (dxion - sink)
@@ -835,14 +873,5 @@ def compute_ts(p: ro.Params, T: TsTables, ZZ, snapshot: int, stored_fcoll, g: di
     tk = np.where(Tk < MAX_TK, (Td + d1 * dzp).astype(f32), Tk).astype(f32)
     tk = np.where(tk < MIN_TK, f32(TCMB * (1 + zp)), tk).astype(f32)
     ts, xa = get_Ts(cm, T, zp, deltax, tk, xn, d2.astype(f32))
-    g["x_e_box_prev"][...] = xn
-    g["Tk_box"][...] = tk
-    g["TS_box"] = ts
-    g["x_e_box"] = xn.copy()
-    out.update(volume_ave_J_alpha=float(np.sum(d2) / n3), volume_ave_xalpha=float(np.sum(xa.astype(np.float64)) / n3),
-               volume_ave_Xheat=float(np.sum(dxheat_dzp) / n3), volume_ave_Xion=float(np.sum(d4) / n3),
-               volume_ave_TS=float(np.sum(ts.astype(np.float64)) / n3),
-               volume_ave_TK=float(np.sum(tk.astype(np.float64)) / n3),
-               volume_ave_xe=float(np.sum(xn.astype(np.float64)) / n3))
-    out["_cells"] = dict(dxheat_dzp=dxheat_dzp, dxion=d4, J_alpha=d2)
-    return out
+    return dict(x_e=xn, Tk=tk, TS=ts, xalpha=xa, J_alpha=d2, dxheat_dzp=dxheat_dzp, dxion=d4)
+
