@@ -308,9 +308,9 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
   if (ctx->d_radii) cudaFree(ctx->d_radii);
-  if (ctx->ts_acc) cudaFree(ctx->ts_acc);
   if (ctx->ts_stage) cudaFree(ctx->ts_stage);
   if (ctx->ts_const) cudaFree(ctx->ts_const);
+  if (ctx->ts_sums) cudaFree(ctx->ts_sums);
   for (void* p : ctx->owned) cudaFree(p);
   prof_resolve(ctx);
   for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);

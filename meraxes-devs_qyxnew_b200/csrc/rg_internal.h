@@ -147,11 +147,11 @@ struct rg_context {
   rg::Tables tables;
   double* d_radii = nullptr;     // device copy of the radius list
   size_t d_radii_elems = 0;
-  double* ts_acc = nullptr;      // ComputeTs per-cell FP64 shell sums [4][N^3]
-  size_t ts_acc_elems = 0;
   float* ts_stage = nullptr;     // ComputeTs source grids staged from host memory [slot][2][padded]
   size_t ts_stage_elems = 0;
-  char* ts_const = nullptr;      // ComputeTs device constants and per-batch coefficients
+  float4* ts_sums = nullptr;     // ComputeTs per-cell shell sums (FP32, scaled) [N^3]
+  size_t ts_sums_elems = 0;
+  char* ts_const = nullptr;      // ComputeTs device constants and per-shell coefficients
   size_t ts_const_elems = 0;
   // profiling
   bool prof_on = false;

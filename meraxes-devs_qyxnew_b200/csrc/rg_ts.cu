@@ -37,9 +37,22 @@ struct KappaSpline {
   double x[KSPL], y[KSPL], b[KSPL], c[KSPL], d[KSPL];
 };
 
+// per-snapshot constants of the per-cell physics (the factors of xcoll, taugp, xalpha_tilde,
+// dT_comp and evolveInt that depend on the redshift only), computed on the host in FP64
+struct TsZConst {
+  double Trad, inv_Trad;       // TCMB (1 + z), z the float redshift
+  double xc_H, xc_e, xc_p;     // T21 / Trad / A10 x {No, N_b0, No} (1 + z)^3   (xcoll_HI/elec/prot)
+  double tgp0;                 // 1.342881e-7 / hubble(z) No (1 + z)^3          (taugp)
+  double xa0;                  // 1.66e11 / (1 + z)                             (xalpha_tilde)
+  double nb0;                  // N_b0 (1 + z)^3                                (evolveInt n_b)
+  double comp0;                // -1.51e-4 / (H(z) / H0) / h Trad^4 / (1 + z)    (dT_comp)
+  double dadia0;               // 3 / (1 + z)
+  double f_H, f_He;
+};
+
 struct TsDev {
   KappaSpline k10, kel, kpH;
-  double No, N_b0, f_H, f_He, h, OMm, OMr, OMl;
+  TsZConst z;
 };
 
 __device__ __forceinline__ double spline_eval(const KappaSpline& s, double x) {
@@ -55,64 +68,47 @@ __device__ __forceinline__ double spline_eval(const KappaSpline& s, double x) {
   return s.y[lo] + dx * (s.b[lo] + dx * (s.c[lo] + dx * s.d[lo]));
 }
 
-// kappa_10 (XRayHeatingFunctions.c:1728-1822)
-__device__ double kappa_10(const TsDev& C, double TK) {
-  const KappaSpline& s = C.k10;
-  double ans;
-  if (log(TK) < s.x[0]) {
-    ans = s.y[0];
-  } else if (log(TK) > s.x[s.n - 1]) {
-    ans = log(exp(s.y[s.n - 1]) * pow(TK / exp(s.x[s.n - 1]), 0.381));
-  } else {
-    ans = spline_eval(s, log(TK));
-  }
-  return exp(ans);
+// log kappa_10 at log T (XRayHeatingFunctions.c:1728-1822): below the table its first value,
+// above it the T^0.381 power law log(exp(y_n) (T / exp(x_n))^0.381) = y_n + 0.381 (log T - x_n)
+__device__ __forceinline__ double log_kappa_10(const KappaSpline& s, double lt) {
+  if (lt < s.x[0]) return s.y[0];
+  if (lt > s.x[s.n - 1]) return s.y[s.n - 1] + 0.381 * (lt - s.x[s.n - 1]);
+  return spline_eval(s, lt);
 }
 
-// kappa_10_elec and kappa_10_pH (XRayHeatingFunctions.c:1827-1966)
-__device__ double kappa_table(const KappaSpline& s, double T) {
-  T = log(T);
-  double ans;
-  if (T < s.x[0]) {
-    ans = s.y[0];
-  } else if (T > s.x[s.n - 1]) {
-    ans = s.y[s.n - 1] + ((s.y[s.n - 1] - s.y[s.n - 2]) / (s.x[s.n - 1] - s.x[s.n - 2]) * (T - s.x[s.n - 1]));
-  } else {
-    ans = spline_eval(s, T);
-  }
-  return exp(ans);
+// log kappa_10_elec / kappa_10_pH at log T (XRayHeatingFunctions.c:1827-1966): linear
+// extrapolation of the last segment above the table
+__device__ __forceinline__ double log_kappa_table(const KappaSpline& s, double lt) {
+  if (lt < s.x[0]) return s.y[0];
+  if (lt > s.x[s.n - 1])
+    return s.y[s.n - 1] + ((s.y[s.n - 1] - s.y[s.n - 2]) / (s.x[s.n - 1] - s.x[s.n - 2]) * (lt - s.x[s.n - 1]));
+  return spline_eval(s, lt);
 }
 
-__device__ __forceinline__ double d_hubble(const TsDev& C, float z) {
-  const double opz = (double)(1.0f + z);
-  return HUBBLE * C.h * sqrt(C.OMm * pow(opz, 3) + C.OMr * pow(opz, 4) + C.OMl);
-}
-
-// xcoll (XRayHeatingFunctions.c:1686-1726)
-__device__ double xcoll(const TsDev& C, double z, double TK, double delta, double xe) {
-  const double Trad = TCMB * (1.0 + z);
-  const double opz3 = pow(1.0 + z, 3.0);
-  const double nH = (1.0 - xe) * C.No * opz3 * (1.0 + delta);
-  const double ne = xe * C.N_b0 * opz3 * (1.0 + delta);
-  const double np = xe * C.No * opz3 * (1.0 + delta);
-  return T21 / Trad * nH * kappa_10(C, TK) / A10_HYPERFINE + T21 / Trad * ne * kappa_table(C.kel, TK) / A10_HYPERFINE +
-         T21 / Trad * np * kappa_table(C.kpH, TK) / A10_HYPERFINE;
-}
-
-// get_Ts and the Wouthuysen-Field coupling (XRayHeatingFunctions.c:1639-1684, 1973-2008); the
-// fixed-point loop is capped at 10000 iterations (a cell that hits the cap counts in *nonconv)
-__device__ float get_Ts(const TsDev& C, float z, float delta, float TK, float xe, float Jalpha, float* curr_xalpha,
+// get_Ts with xcoll and the Wouthuysen-Field coupling (XRayHeatingFunctions.c:1639-1726,
+// 1973-2008).  The factors that do not change across the fixed-point iterations (xcoll, the
+// S_alpha terms in T_K only, xi) are evaluated once per cell.  The loop is capped at 10000
+// iterations; a cell that reaches the cap counts in *nonconv.
+__device__ float get_Ts(const TsDev& C, float delta, float TK, float xe, float Jalpha, float* curr_xalpha,
                         int* nonconv) {
-  const double Trad = TCMB * (1.0 + (double)z);
-  const double xc = xcoll(C, (double)z, (double)TK, (double)delta, (double)xe);
-  double TS, TSinv;
+  const TsZConst& Z = C.z;
+  const double tk = (double)TK, d1 = 1.0 + (double)delta, x = (double)xe;
+  const double lt = log(tk);
+  const double xc = Z.xc_H * (1.0 - x) * d1 * exp(log_kappa_10(C.k10, lt)) +
+                    Z.xc_e * x * d1 * exp(log_kappa_table(C.kel, lt)) +
+                    Z.xc_p * x * d1 * exp(log_kappa_table(C.kpH, lt));
+  const double itk = 1.0 / tk;
+  double TS;
   if ((double)Jalpha > 1.0e-20) {
-    TS = Trad;
+    const double tgp = Z.tgp0 * d1 * (1.0 - x);
+    const double xi = cbrt(1.0e-7 * tgp * itk * itk);
+    const double den = 1.0 + 2.98394 * xi + 1.53583 * xi * xi + 3.85289 * xi * xi * xi;
+    const double sa = 1.0 - 0.0631789 * itk + 0.115995 * itk * itk;    // S_alpha terms in T_K only
+    const double sb = (-0.401403 + 0.336463 * itk) * itk;                 // times 1 / T_S
+    const double xaj = Z.xa0 * (double)Jalpha / den;
+    const double ctc = 0.405535 * itk;
+    TS = Z.Trad;
     double TSold = 0.0, xa_tilde = 0.0;
-    const double zz = (double)z;
-    const double tgp = 1.342881e-7 / d_hubble(C, (float)zz) * C.No * pow(1 + zz, 3) * (1.0 + (double)delta) *
-                       (1.0 - (double)xe);
-    const double tk = (double)TK;
     int it = 0;
     while (fabs(TS - TSold) / TS > 1.0e-3) {
       if (++it > 10000) {
@@ -120,43 +116,33 @@ __device__ float get_Ts(const TsDev& C, float z, float delta, float TK, float xe
         break;
       }
       TSold = TS;
-      // Salpha_tilde and xalpha_tilde
-      const double xi = pow(1.0e-7 * tgp / tk / tk, 1.0 / 3.0);
-      double st = 1.0 - 0.0631789 / tk + 0.115995 / tk / tk - 0.401403 / TS / tk;
-      st += 0.336463 / TS / tk / tk;
-      st /= 1.0 + 2.98394 * xi + 1.53583 * xi * xi + 3.85289 * xi * xi * xi;
-      xa_tilde = 1.66e11 / (1.0 + zz) * st * (double)Jalpha;
-      // Tc_eff
-      double tce = 1.0 / tk + 0.405535 / tk * (1.0 / TS - 1.0 / tk);
-      tce = 1.0 / tce;
-      TSinv = (1.0 / Trad + xa_tilde / tce + xc / tk) / (1.0 + xa_tilde + xc);
-      TS = 1.0 / TSinv;
+      const double u = 1.0 / TS;
+      xa_tilde = xaj * (sa + sb * u);
+      const double tce_inv = itk + ctc * (u - itk);                        // 1 / Tc_eff
+      TS = (1.0 + xa_tilde + xc) / (Z.inv_Trad + xa_tilde * tce_inv + xc * itk);
     }
     *curr_xalpha = (float)xa_tilde;
   } else {
-    TSinv = (1.0 / Trad + xc / (double)TK) / (1.0 + xc);
-    TS = 1.0 / TSinv;
+    TS = (1.0 + xc) / (Z.inv_Trad + xc * itk);
     *curr_xalpha = 0;
   }
   if (TS < 0.) TS = fabs(TS);
   return (float)TS;
 }
 
-// alpha_A (XRayHeatingFunctions.c:1576-1584)
-__device__ double alpha_A(double T) {
-  const double logT = log(T / (double)1.1604505e4);
-  return exp(-28.6130338 - 0.72411256 * logT - 2.02604473e-2 * pow(logT, 2) - 2.38086188e-3 * pow(logT, 3) -
-             3.21260521e-4 * pow(logT, 4) - 1.42150291e-5 * pow(logT, 5) + 4.98910892e-6 * pow(logT, 6) +
-             5.75561414e-7 * pow(logT, 7) - 1.85676704e-8 * pow(logT, 8) - 3.07113524e-9 * pow(logT, 9));
-}
-
-// dT_comp (XRayHeatingFunctions.c:1564-1573)
-__device__ double dT_comp(const TsDev& C, double z, double TK, double xe) {
-  const double Trad = TCMB * (1.0 + z);
-  double ans = (-1.51e-4) * (xe / (1.0 + xe + C.f_He)) / (d_hubble(C, (float)z) / (HUBBLE * C.h)) / C.h *
-               pow(Trad, 4.0) / (1.0 + z);
-  ans *= Trad - TK;
-  return ans;
+// alpha_A (XRayHeatingFunctions.c:1576-1584): exp of a degree-9 polynomial in
+// log(T / 1.1604505e4), evaluated by Horner's rule
+__device__ __forceinline__ double alpha_A(double T) {
+  const double l = log(T / 1.1604505e4);
+  const double poly =
+      -28.6130338 +
+      l * (-0.72411256 +
+           l * (-2.02604473e-2 +
+                l * (-2.38086188e-3 +
+                     l * (-3.21260521e-4 +
+                          l * (-1.42150291e-5 +
+                               l * (4.98910892e-6 + l * (5.75561414e-7 + l * (-1.85676704e-8 + l * -3.07113524e-9))))))));
+  return exp(poly);
 }
 
 // ---------------------------------------------------------------------------
@@ -264,146 +250,208 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<
 }
 
 // ---------------------------------------------------------------------------
-// shell z pass: c2r of the sfr and xray grids of every shell of the batch, accumulated per cell
-// into the four evolveInt sums (FP32 within a batch, FP64 across batches)
+// per-cell evolution (evolveInt + the Euler step + get_Ts, ComputeTs.c:1171-1407)
 
-struct TsCoef {
-  // per shell of the batch: P/Q of the x_e interpolation for heat, ion, lya (scaled), and the
-  // scaled stellar Lyman-alpha coefficient; fi_k = P_k[lo] + (x_e - X[lo]) Q_k[lo]
-  float P[TS_KB][3][x_int_NXHII];
-  float Q[TS_KB][3][x_int_NXHII];
-  float cstar[TS_KB];
+struct TsEvolve {
+  double zp, dzp, dt_dzp, growth, dgrowth, const_zp, conv_star;
+  double heat_conv;            // dt_dzp 2 / 3 / k_B
+  int no_light;
+};
+
+// One cell: sums[0..3] = the four evolveInt shell sums (heat, ion, lya, stellar lya) before
+// their snapshot prefactors; updates x_e and T_K, returns T_S and adds the cell to acc[0..6].
+__device__ __forceinline__ void evolve_cell(const TsDev& C, const TsEvolve& e, float delta, float xef, float tk0,
+                                            const double (&sums)[4], float* xn_out, float* tk_out, float* ts_out,
+                                            double (&acc)[TS_NSUM], int* nc) {
+  const TsZConst& Z = C.z;
+  const double x_e = (double)xef, T = (double)tk0;
+  const double n_b = Z.nb0 * (double)(1.0f + delta);
+  double dxheat_dt = 0, dxion_src = 0, dxlya = 0, dstarlya = 0;
+  if (!e.no_light) {
+    dxheat_dt = sums[0] * e.const_zp;
+    dxion_src = sums[1] * e.const_zp;
+    dxlya = sums[2] * (e.const_zp * n_b);
+    dstarlya = sums[3] * e.conv_star;
+  }
+  const double inv1x = 1.0 / (1.0 + x_e);
+  const double dxion_sink = alpha_A(T) * CLUMPING_FACTOR * x_e * x_e * Z.f_H * n_b;
+  const double dxe_dzp = e.dt_dzp * (dxion_src - dxion_sink);
+  double dadia = Z.dadia0;
+  if (fabs((double)delta) > FRACT_FLOAT_ERR) {
+    const double dl = (double)delta;
+    dadia += e.dgrowth * dl / (1.0 + e.growth * dl);      // dgrowth / (1 / delta + growth)
+  }
+  dadia *= (2.0 / 3.0) * T;
+  const double dspec = -dxe_dzp * T * inv1x;
+  const double dcomp = Z.comp0 * (x_e / (1.0 + x_e + Z.f_He)) * (Z.Trad - T);
+  const double dxheat_dzp = dxheat_dt * e.heat_conv * inv1x;
+  const double d1 = dxheat_dzp + dcomp + dspec + dadia;
+  const double d2 = dxlya + dstarlya;
+  const double d4 = e.dt_dzp * dxion_src;
+  float xn = (float)((double)xef + dxe_dzp * e.dzp);
+  if (xn > 1)
+    xn = (float)(1 - FRACT_FLOAT_ERR);
+  else if (xn < 0)
+    xn = 0;
+  float tk = tk0;
+  if (tk < MAX_TK) tk = (float)((double)tk + d1 * e.dzp);
+  if (tk < MIN_TK) tk = (float)(TCMB * (1 + e.zp));
+  float xa;
+  const float ts = get_Ts(C, delta, tk, xn, (float)d2, &xa, nc);
+  *xn_out = xn;
+  *tk_out = tk;
+  *ts_out = ts;
+  acc[0] += d2;
+  acc[1] += (double)xa;
+  acc[2] += dxheat_dzp;
+  acc[3] += d4;
+  acc[4] += (double)ts;
+  acc[5] += (double)tk;
+  acc[6] += (double)xn;
+}
+
+// ---------------------------------------------------------------------------
+// shell z pass: for every shell r the c2r along z of its sfr and X-ray grids, accumulated per
+// cell into the four evolveInt shell sums in registers over all shells, then stored once as a
+// float4 per cell.  Two shells share one complex line (the two-for-one c2r of two real rows:
+// shell r in the real part, shell r + 1 in the imaginary part; both rows are the same grid,
+// filtered at neighbouring radii).
+//
+// Per shell: P_k[m], Q_k[m] (k = heat, ion, lya; m = x_e node) so that the cell's term is
+// xray x (P_k[lo] + (x_e - X[lo]) Q_k[lo]), and cstar for max(sfr, 0); all scaled by a power of
+// two per sum kind so FP32 keeps its range (the scale is undone in FP64 by the update kernel).
+
+struct TsShellCoef {
+  float P[3][x_int_NXHII];
+  float Q[3][x_int_NXHII];
+  float cstar;
+  float pad;
+};
+
+struct TsZev {
+  int nS;
   float X[x_int_NXHII];           // x_int_XHII (float, as in the reference)
-  double inv_scale[4];            // undo the FP32 scaling when flushing to FP64
-  int nr;
-  int first;                      // first batch: the FP64 sums start at zero
+  double inv_scale[4];            // undo the FP32 scaling
 };
 
 template <int N>
 struct TsZ {
   using PL = Plan8<N>;
   static constexpr int T = PL::T;
-  static constexpr int Q = pow2_div(N / 2, cmax(256 / T, 1));
-  static constexpr int NTH = T * Q;
   static constexpr int V = N / T;            // 8
   static constexpr int R0 = PL::R[0];
+  static constexpr int Q = pow2_div(N, cmax(256 / T, 4));   // rows per block
+  static constexpr int NTH = T * Q;
+  static constexpr int MINB = NTH >= 512 ? 1 : 512 / NTH;   // 2 blocks of 256: at most 128 registers
   static constexpr size_t smem() { return sizeof(cf) * (N + (size_t)line_buf_r0<N, R0, Q>()); }
 };
 
+// complex line of rows (x, y) of two shells' Hermitian halves a, b (b may be null)
 template <int N>
-__global__ void __launch_bounds__(TsZ<N>::NTH, RG_MINB(TsZ<N>::NTH))
-    k_ts_z(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw, const TsCoef* __restrict__ gco,
-           const float* __restrict__ xe_box, double* __restrict__ acc_g) {
+__device__ __forceinline__ cf pair_c2r_input(const cf* __restrict__ a, const cf* __restrict__ b, size_t col, int p) {
+  const int k = p <= N / 2 ? p : N - p;
+  const size_t o = col + (size_t)k * N * N;
+  const float2 A = __ldg(reinterpret_cast<const float2*>(a + o));
+  float2 B = make_float2(0.f, 0.f);
+  if (b) B = __ldg(reinterpret_cast<const float2*>(b + o));
+  if (p == 0 || p == N / 2) return cf{A.x, B.x};
+  if (p < N / 2) return cf{A.x - B.y, A.y + B.x};
+  return cf{A.x + B.y, B.x - A.y};
+}
+
+template <int N>
+__global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
+    k_ts_zsum(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw,
+              const TsShellCoef* __restrict__ gco, TsZev zv, const float* __restrict__ xe_prev,
+              float4* __restrict__ sums) {
   using Z = TsZ<N>;
   using PL = typename Z::PL;
-  constexpr int T = Z::T, Q = Z::Q, V = Z::V;
+  constexpr int Q = Z::Q, V = Z::V;
   constexpr int PADW = 2 * (N / 2 + 1);
-  constexpr size_t N3 = (size_t)N * N * N;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
   cf* xbuf = smem + N;
-  __shared__ TsCoef co;
-  const int x = blockIdx.y, y0 = blockIdx.x * 2 * Q;
-  const int q = threadIdx.x % Q, t = threadIdx.x / Q;
+  __shared__ TsShellCoef sc[2];
+  const int x = blockIdx.y, y = blockIdx.x * Q + threadIdx.x % Q;
+  const int t = threadIdx.x / Q;
   load_twiddles<N>(s_tw, g_tw);
-  {
-    const int* src = reinterpret_cast<const int*>(gco);
-    int* dst = reinterpret_cast<int*>(&co);
-    for (int i = threadIdx.x; i < (int)(sizeof(TsCoef) / sizeof(int)); i += Z::NTH) dst[i] = src[i];
-  }
-  __syncthreads();
-  // cells of this thread: rows y0 + 2q + h, positions last_pos(t, s)
-  float dxe[2 * V];
-  uint64_t lopack = 0;
+  const size_t row = (size_t)x * N + y;
+  // this thread's cells: z = last_pos(t, s); x_e interpolation node and offset
+  // (ComputeTs.c:1198-1209)
+  float dxe[V];
+  uint32_t lopack = 0;
 #pragma unroll
-  for (int s = 0; s < V; ++s) {
-    const int z = last_pos<PL>(t, s);
+  for (int sl = 0; sl < V; ++sl) {
+    double xc = (double)__ldg(xe_prev + row * PADW + last_pos<PL>(t, sl));
+    if (xc > (double)zv.X[x_int_NXHII - 1] * 0.999)
+      xc = (double)zv.X[x_int_NXHII - 1] * 0.999;
+    else if (xc < (double)zv.X[0])
+      xc = 1.001 * (double)zv.X[0];
+    // locate_xHII_index: the last node not above x_e (constant indices keep zv in the
+    // parameter bank)
+    const float xf = (float)xc;
+    int m = 0;
+    float xm = zv.X[0];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      double xc = (double)__ldg(xe_box + ((size_t)x * N + y0 + 2 * q + h) * PADW + z);
-      // ComputeTs.c:1198-1208
-      if (xc > (double)co.X[x_int_NXHII - 1] * 0.999)
-        xc = (double)co.X[x_int_NXHII - 1] * 0.999;
-      else if (xc < (double)co.X[0])
-        xc = 1.001 * (double)co.X[0];
-      const float xf = (float)xc;
-      int m = x_int_NXHII - 1;
-      while (xf < co.X[m]) m--;
-      lopack |= (uint64_t)m << (4 * (2 * s + h));
-      dxe[2 * s + h] = (float)(xc - (double)co.X[m]);
-    }
-  }
-  float a_heat[2 * V], a_ion[2 * V], a_lya[2 * V], a_star[2 * V];
-#pragma unroll
-  for (int c = 0; c < 2 * V; ++c) a_heat[c] = a_ion[c] = a_lya[c] = a_star[c] = 0.f;
-  const size_t colpair = (size_t)x * N + y0 + 2 * q;
-  auto addr = [&](int p) { return line_addr_r0<Z::R0, Q>(p, q); };
-  for (int r = 0; r < co.nr; ++r) {
-    // sfr: stellar Lyman-alpha sum, SFR clamped at 0 (ComputeTs.c:700)
-    const cf* gs = work + ((size_t)r * 2 + 0) * stride;
-    const float cst = co.cstar[r];
-    line_fft_p<PL, true>(
-        t, xbuf, s_tw, [&](int p, int) { return build_c2r_input<N>(gs, colpair, p); }, addr,
-        [&](int, cf v, int sl) {
-          a_star[2 * sl] = fmaf(fmaxf(v.x, 0.f), cst, a_star[2 * sl]);
-          a_star[2 * sl + 1] = fmaf(fmaxf(v.y, 0.f), cst, a_star[2 * sl + 1]);
-        });
-    // xray: heating, ionisation and Lyman-alpha integrands, not clamped
-    const cf* gx = work + ((size_t)r * 2 + 1) * stride;
-    line_fft_p<PL, true>(
-        t, xbuf, s_tw, [&](int p, int) { return build_c2r_input<N>(gx, colpair, p); }, addr,
-        [&](int, cf v, int sl) {
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int c = 2 * sl + h;
-            const int lo = (int)((lopack >> (4 * c)) & 15u);
-            const float d = dxe[c];
-            const float xr = h ? v.y : v.x;
-            a_heat[c] = fmaf(xr, fmaf(d, co.Q[r][0][lo], co.P[r][0][lo]), a_heat[c]);
-            a_ion[c] = fmaf(xr, fmaf(d, co.Q[r][1][lo], co.P[r][1][lo]), a_ion[c]);
-            a_lya[c] = fmaf(xr, fmaf(d, co.Q[r][2][lo], co.P[r][2][lo]), a_lya[c]);
-          }
-        });
-  }
-  // flush to the FP64 sums
-#pragma unroll
-  for (int s = 0; s < V; ++s) {
-    const int z = last_pos<PL>(t, s);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int c = 2 * s + h;
-      const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
-      const double v0 = (double)a_heat[c] * co.inv_scale[0], v1 = (double)a_ion[c] * co.inv_scale[1];
-      const double v2 = (double)a_lya[c] * co.inv_scale[2], v3 = (double)a_star[c] * co.inv_scale[3];
-      if (co.first) {
-        acc_g[ir] = v0;
-        acc_g[N3 + ir] = v1;
-        acc_g[2 * N3 + ir] = v2;
-        acc_g[3 * N3 + ir] = v3;
-      } else {
-        acc_g[ir] += v0;
-        acc_g[N3 + ir] += v1;
-        acc_g[2 * N3 + ir] += v2;
-        acc_g[3 * N3 + ir] += v3;
+    for (int j = 1; j < x_int_NXHII; ++j)
+      if (!(xf < zv.X[j])) {
+        m = j;
+        xm = zv.X[j];
       }
+    lopack |= (uint32_t)m << (4 * sl);
+    dxe[sl] = (float)(xc - (double)xm);
+  }
+  float a_heat[V], a_ion[V], a_lya[V], a_star[V];
+#pragma unroll
+  for (int sl = 0; sl < V; ++sl) a_heat[sl] = a_ion[sl] = a_lya[sl] = a_star[sl] = 0.f;
+  auto addr = [&](int p) { return line_addr_r0<Z::R0, Q>(p, threadIdx.x % Q); };
+  for (int r = 0; r < zv.nS; r += 2) {
+    const bool two = r + 1 < zv.nS;
+    __syncthreads();  // readers of the previous pair's coefficients are done
+    {
+      const int* src = reinterpret_cast<const int*>(gco + r);
+      int* dst = reinterpret_cast<int*>(sc);
+      const int nwords = (two ? 2 : 1) * (int)(sizeof(TsShellCoef) / sizeof(int));
+      for (int i = threadIdx.x; i < (int)(2 * sizeof(TsShellCoef) / sizeof(int)); i += Z::NTH)
+        dst[i] = i < nwords ? src[i] : 0;
+    }
+    __syncthreads();
+    // sfr: stellar Lyman-alpha sum, SFR clamped at 0 (ComputeTs.c:700)
+    {
+      const cf* ga = work + ((size_t)r * 2 + 0) * stride;
+      const cf* gb = two ? work + ((size_t)(r + 1) * 2 + 0) * stride : nullptr;
+      const float c0 = sc[0].cstar, c1 = sc[1].cstar;
+      line_fft_p<PL, true>(
+          t, xbuf, s_tw, [&](int p, int) { return pair_c2r_input<N>(ga, gb, row, p); }, addr,
+          [&](int, cf v, int sl) { a_star[sl] += fmaxf(v.x, 0.f) * c0 + fmaxf(v.y, 0.f) * c1; });
+    }
+    // X-ray: heating, ionisation and Lyman-alpha integrands, not clamped
+    {
+      const cf* ga = work + ((size_t)r * 2 + 1) * stride;
+      const cf* gb = two ? work + ((size_t)(r + 1) * 2 + 1) * stride : nullptr;
+      line_fft_p<PL, true>(
+          t, xbuf, s_tw, [&](int p, int) { return pair_c2r_input<N>(ga, gb, row, p); }, addr,
+          [&](int, cf v, int sl) {
+            const int lo = (int)((lopack >> (4 * sl)) & 15u);
+            const float d = dxe[sl];
+            a_heat[sl] += v.x * fmaf(d, sc[0].Q[0][lo], sc[0].P[0][lo]) + v.y * fmaf(d, sc[1].Q[0][lo], sc[1].P[0][lo]);
+            a_ion[sl] += v.x * fmaf(d, sc[0].Q[1][lo], sc[0].P[1][lo]) + v.y * fmaf(d, sc[1].Q[1][lo], sc[1].P[1][lo]);
+            a_lya[sl] += v.x * fmaf(d, sc[0].Q[2][lo], sc[0].P[2][lo]) + v.y * fmaf(d, sc[1].Q[2][lo], sc[1].P[2][lo]);
+          });
     }
   }
+#pragma unroll
+  for (int sl = 0; sl < V; ++sl)
+    sums[row * N + last_pos<PL>(t, sl)] = make_float4(a_heat[sl], a_ion[sl], a_lya[sl], a_star[sl]);
 }
 
-// ---------------------------------------------------------------------------
-// per-cell evolution (evolveInt + the Euler step + get_Ts, ComputeTs.c:1171-1407)
-
-struct TsEvolve {
-  float zp_f;
-  double zp, dzp, dt_dzp, growth, dgrowth, const_zp, conv_star;
-  int no_light;
-};
-
-__global__ void __launch_bounds__(256) k_ts_evolve(const TsDev* __restrict__ gC, TsEvolve e, int n,
-                                                   const double* __restrict__ acc_g, const float* __restrict__ deltax,
-                                                   float* __restrict__ xe_prev, float* __restrict__ xe_box,
-                                                   float* __restrict__ Tk, float* __restrict__ TS,
-                                                   double* __restrict__ partials, int* __restrict__ nonconv) {
+// the per-cell update (ComputeTs.c:1171-1407) from the shell sums; sums == nullptr: no light
+__global__ void __launch_bounds__(256) k_ts_evolve(const TsDev* __restrict__ gC, TsEvolve e, double4 inv_scale, int n,
+                                                   const float4* __restrict__ sums,
+                                                   const float* __restrict__ deltax, float* __restrict__ xe_prev,
+                                                   float* __restrict__ xe_box, float* __restrict__ Tk,
+                                                   float* __restrict__ TS, double* __restrict__ partials,
+                                                   int* __restrict__ nonconv) {
   __shared__ TsDev C;
   {
     const int* src = reinterpret_cast<const int*>(gC);
@@ -412,7 +460,7 @@ __global__ void __launch_bounds__(256) k_ts_evolve(const TsDev* __restrict__ gC,
   }
   __syncthreads();
   const int padw = 2 * (n / 2 + 1);
-  const size_t rows = (size_t)n * n, n3 = rows * n;
+  const size_t rows = (size_t)n * n;
   double acc[TS_NSUM];
 #pragma unroll
   for (int i = 0; i < TS_NSUM; ++i) acc[i] = 0.0;
@@ -420,56 +468,27 @@ __global__ void __launch_bounds__(256) k_ts_evolve(const TsDev* __restrict__ gC,
   for (size_t row = blockIdx.x; row < rows; row += gridDim.x)
     for (int z = threadIdx.x; z < n; z += blockDim.x) {
       const size_t ir = row * n + z, ip = row * padw + z;
-      const float delta = deltax[ip];
-      const float xef = xe_prev[ip];
-      const double x_e = (double)xef, T = (double)Tk[ir];
-      const double n_b = C.N_b0 * pow((double)(1.0f + e.zp_f), 3) * (double)(1.0f + delta);
-      double dxheat_dt = 0, dxion_src = 0, dxlya = 0, dstarlya = 0;
-      if (!e.no_light) {
-        dxheat_dt = acc_g[ir] * e.const_zp;
-        dxion_src = acc_g[n3 + ir] * e.const_zp;
-        dxlya = acc_g[2 * n3 + ir] * (e.const_zp * n_b);
-        dstarlya = acc_g[3 * n3 + ir] * e.conv_star;
+      double sm[4] = {0.0, 0.0, 0.0, 0.0};
+      if (sums) {
+        const float4 v = __ldg(sums + ir);
+        sm[0] = (double)v.x * inv_scale.x;
+        sm[1] = (double)v.y * inv_scale.y;
+        sm[2] = (double)v.z * inv_scale.z;
+        sm[3] = (double)v.w * inv_scale.w;
       }
-      const double dxion_sink = alpha_A(T) * CLUMPING_FACTOR * x_e * x_e * C.f_H * n_b;
-      const double dxe_dzp = e.dt_dzp * (dxion_src - dxion_sink);
-      double dadia = 3 / (1.0 + (double)e.zp_f);
-      if (fabs((double)delta) > FRACT_FLOAT_ERR) dadia += e.dgrowth / (1.0 / (double)delta + e.growth);
-      dadia *= (2.0 / 3.0) * T;
-      const double dspec = -dxe_dzp * T / (1 + x_e);
-      const double dcomp = dT_comp(C, (double)e.zp_f, T, x_e);
-      const double dxheat_dzp = dxheat_dt * e.dt_dzp * 2.0 / 3.0 / BOLTZMANN / (1.0 + x_e);
-      const double d1 = dxheat_dzp + dcomp + dspec + dadia;
-      const double d2 = dxlya + dstarlya;
-      const double d4 = e.dt_dzp * dxion_src;
-      float xn = (float)((double)xef + dxe_dzp * e.dzp);
-      if (xn > 1)
-        xn = (float)(1 - FRACT_FLOAT_ERR);
-      else if (xn < 0)
-        xn = 0;
-      float tk = Tk[ir];
-      if (tk < MAX_TK) tk = (float)((double)tk + d1 * e.dzp);
-      if (tk < MIN_TK) tk = (float)(TCMB * (1 + e.zp));
-      float xa;
-      const float ts = get_Ts(C, e.zp_f, delta, tk, xn, (float)d2, &xa, &nc);
+      float xn, tk, ts;
+      evolve_cell(C, e, __ldg(deltax + ip), xe_prev[ip], Tk[ir], sm, &xn, &tk, &ts, acc, &nc);
       xe_prev[ip] = xn;
       xe_box[ip] = xn;
       Tk[ir] = tk;
       TS[ir] = ts;
-      acc[0] += d2;
-      acc[1] += (double)xa;
-      acc[2] += dxheat_dzp;
-      acc[3] += d4;
-      acc[4] += (double)ts;
-      acc[5] += (double)tk;
-      acc[6] += (double)xn;
     }
   if (nc) atomicAdd(nonconv, nc);
   block_sum_dyn<TS_NSUM>(acc, partials + (size_t)blockIdx.x * TS_NSUM);
 }
 
 // homogeneous branch (ComputeTs.c:252-278) and the closing averages (:1459-1494)
-__global__ void __launch_bounds__(256) k_ts_homog(const TsDev* __restrict__ gC, float zp_f, float xe0, float TK0,
+__global__ void __launch_bounds__(256) k_ts_homog(const TsDev* __restrict__ gC, float xe0, float TK0,
                                                   float cT_ad, int n, const float* __restrict__ deltax,
                                                   float* __restrict__ xe_prev, float* __restrict__ xe_box,
                                                   float* __restrict__ Tk, float* __restrict__ TS,
@@ -493,7 +512,7 @@ __global__ void __launch_bounds__(256) k_ts_homog(const TsDev* __restrict__ gC, 
       const float delta = deltax[ip];
       const float tk = (float)((double)TK0 * (1.0 + (double)(cT_ad * delta)));
       float xa;
-      const float ts = get_Ts(C, zp_f, delta, tk, xe0, 0.f, &xa, &nc);
+      const float ts = get_Ts(C, delta, tk, xe0, 0.f, &xa, &nc);
       xe_prev[ip] = xe0;
       xe_box[ip] = xe0;
       Tk[ir] = tk;
@@ -536,19 +555,19 @@ static int ensure_mem(rg_context* ctx, T** ptr, size_t* have, size_t need) {
   return RG_OK;
 }
 
+// x and y passes of a batch of shells: work_base + (j * 2 + g) * stride, j < bt.nr
 template <int N>
-static int launch_ts_batch(rg_context* ctx, const cf* spec, cf* work, size_t stride, const TsBatch& bt,
-                           const float* wtab, int wpitch, const TsCoef* d_co, const float* xe_box, double* acc,
-                           cudaStream_t st) {
+static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
+                        const float* wtab, int wpitch, cudaStream_t st) {
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
-  const double nzc = (double)C::NZ * N * N, n3 = (double)N * N * N;
+  const double nzc = (double)C::NZ * N * N;
   const size_t smx = sizeof(cf) * (N + (size_t)line_buf<N, C::BX>());
   RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_x<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
   prof_begin(ctx, "ts_x_c2c_combine_window", st);
-  k_ts_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smx, st>>>(spec, stride, work, bt, wtab, wpitch, tw);
+  k_ts_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smx, st>>>(spec, stride, work_base, bt, wtab, wpitch, tw);
   double src_reads = 0;
   for (int r = 0; r < bt.nr; ++r) src_reads += bt.nk[r];
   prof_end(ctx, 2 * 8.0 * nzc * (src_reads + bt.nr), st);
@@ -556,34 +575,51 @@ static int launch_ts_batch(rg_context* ctx, const cf* spec, cf* work, size_t str
   const size_t smy = sizeof(cf) * (N + (size_t)C::BY * C::PITCH_P);
   RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_pass_y<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
   prof_begin(ctx, "ts_y_c2c", st);
-  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, 2 * bt.nr), C::T * C::BY, smy, st>>>(work, stride, tw);
+  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, 2 * bt.nr), C::T * C::BY, smy, st>>>(work_base, stride, tw);
   prof_end(ctx, 2 * bt.nr * 16.0 * nzc, st);
-  RG_CUDA_TRY(ctx, cudaGetLastError());
-  using Z = TsZ<N>;
-  const size_t smz = Z::smem();
-  RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_z<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
-  prof_begin(ctx, "ts_z_c2r_accumulate", st);
-  k_ts_z<N><<<dim3(N / (2 * Z::Q), N), Z::NTH, smz, st>>>(work, stride, tw, d_co, xe_box, acc);
-  // Hermitian halves of both grids per shell, x_e read, four FP64 sums read (after the first
-  // batch) and written
-  prof_end(ctx, bt.nr * 2 * 8.0 * nzc + 4.0 * n3 + 32.0 * n3 * 2, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 
-static int ts_batch(rg_context* ctx, int n, const cf* spec, cf* work, size_t stride, const TsBatch& bt,
-                    const float* wtab, int wpitch, const TsCoef* d_co, const float* xe_box, double* acc,
-                    cudaStream_t st) {
-  switch (n) {
-    case 8: return launch_ts_batch<8>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    case 16: return launch_ts_batch<16>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    case 32: return launch_ts_batch<32>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    case 64: return launch_ts_batch<64>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    case 128: return launch_ts_batch<128>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    case 256: return launch_ts_batch<256>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    case 512: return launch_ts_batch<512>(ctx, spec, work, stride, bt, wtab, wpitch, d_co, xe_box, acc, st);
-    default: return set_error(ctx, RG_EUNSUPPORTED, "ComputeTs needs a power-of-two ReionGridDim");
+// the z pass over all nS shells: per-cell shell sums
+template <int N>
+static int launch_ts_zsum(rg_context* ctx, const cf* work, size_t stride, const TsShellCoef* d_co, const TsZev& zv,
+                          const float* xe_prev, float4* sums, cudaStream_t st) {
+  const cf* tw;
+  int rc = twiddles_for(ctx, N, &tw);
+  if (rc) return rc;
+  using Z = TsZ<N>;
+  const double n3 = (double)N * N * N, nzc = (double)(N / 2 + 1) * N * N;
+  const size_t smz = Z::smem();
+  RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_zsum<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+  prof_begin(ctx, "ts_z_c2r_sums", st);
+  k_ts_zsum<N><<<dim3(N / Z::Q, N), Z::NTH, smz, st>>>(work, stride, tw, d_co, zv, xe_prev, sums);
+  // Hermitian halves of both grids of every shell, x_e read, four float sums written
+  prof_end(ctx, zv.nS * 2 * 8.0 * nzc + 4.0 * n3 + 16.0 * n3, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  return RG_OK;
+}
+
+#define RG_TS_DISPATCH(n, call)                                                           \
+  switch (n) {                                                                            \
+    case 8: { constexpr int NN = 8; return call; }                                        \
+    case 16: { constexpr int NN = 16; return call; }                                      \
+    case 32: { constexpr int NN = 32; return call; }                                      \
+    case 64: { constexpr int NN = 64; return call; }                                      \
+    case 128: { constexpr int NN = 128; return call; }                                    \
+    case 256: { constexpr int NN = 256; return call; }                                    \
+    case 512: { constexpr int NN = 512; return call; }                                    \
+    default: return set_error(ctx, RG_EUNSUPPORTED, "ComputeTs needs a power-of-two ReionGridDim"); \
   }
+
+static int ts_xy(rg_context* ctx, int n, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
+                 const float* wtab, int wpitch, cudaStream_t st) {
+  RG_TS_DISPATCH(n, launch_ts_xy<NN>(ctx, spec, work_base, stride, bt, wtab, wpitch, st));
+}
+
+static int ts_zsum(rg_context* ctx, int n, const cf* work, size_t stride, const TsShellCoef* d_co, const TsZev& zv,
+                   const float* xe_prev, float4* sums, cudaStream_t st) {
+  RG_TS_DISPATCH(n, launch_ts_zsum<NN>(ctx, work, stride, d_co, zv, xe_prev, sums, st));
 }
 
 static double pow2_scale(double maxabs) {
@@ -610,23 +646,35 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   fill_spline(ctx->tables.k10, ctx->tables.k10_lT, ctx->tables.k10_lk, &hc.k10);
   fill_spline(ctx->tables.kel, ctx->tables.kel_lT, ctx->tables.kel_lk, &hc.kel);
   fill_spline(ctx->tables.kpH, ctx->tables.kpH_lT, ctx->tables.kpH_lk, &hc.kpH);
-  hc.No = cm.No;
-  hc.N_b0 = cm.N_b0;
-  hc.f_H = cm.f_H;
-  hc.f_He = cm.f_He;
-  hc.h = p->Hubble_h;
-  hc.OMm = p->OmegaM;
-  hc.OMr = p->OmegaR;
-  hc.OMl = p->OmegaLambda;
-  // device constants, the non-convergence counter and the per-batch coefficients live in one
-  // context buffer: [TsDev][int + pad][TsCoef x batches]
+  {
+    // per-redshift factors of xcoll / taugp / xalpha_tilde / dT_comp / evolveInt; the C passes
+    // the redshift to them as a float
+    const float zf = (float)zp;
+    const double z = (double)zf;
+    TsZConst& Z = hc.z;
+    Z.Trad = TCMB * (1.0 + z);
+    Z.inv_Trad = 1.0 / Z.Trad;
+    const double opz3 = std::pow(1.0 + z, 3.0);
+    Z.xc_H = T21 / Z.Trad * cm.No * opz3 / A10_HYPERFINE;
+    Z.xc_e = T21 / Z.Trad * cm.N_b0 * opz3 / A10_HYPERFINE;
+    Z.xc_p = Z.xc_H;
+    Z.tgp0 = 1.342881e-7 / cm.hubble(zf) * cm.No * opz3;
+    Z.xa0 = 1.66e11 / (1.0 + z);
+    Z.nb0 = cm.N_b0 * std::pow((double)(1.0f + zf), 3);
+    Z.comp0 = (-1.51e-4) / (cm.hubble(zf) / (HUBBLE * p->Hubble_h)) / p->Hubble_h * std::pow(Z.Trad, 4.0) / (1.0 + z);
+    Z.dadia0 = 3 / (1.0 + z);
+    Z.f_H = cm.f_H;
+    Z.f_He = cm.f_He;
+  }
+  // device constants, the non-convergence counter and the per-shell coefficients live in one
+  // context buffer: [TsDev][int + pad][TsShellCoef x shells]
   const int nS_all = p->TsNumFilterSteps;
-  const int nbatch_max = (nS_all + TS_KB - 1) / TS_KB;
   const size_t off_co = (sizeof(TsDev) + 16 + 255) / 256 * 256;
-  if ((rc = ensure_mem(ctx, &ctx->ts_const, &ctx->ts_const_elems, off_co + sizeof(TsCoef) * nbatch_max))) return rc;
+  if ((rc = ensure_mem(ctx, &ctx->ts_const, &ctx->ts_const_elems, off_co + sizeof(TsShellCoef) * (nS_all + 1))))
+    return rc;
   TsDev* d_hc = reinterpret_cast<TsDev*>(ctx->ts_const);
   int* d_nonconv = reinterpret_cast<int*>(ctx->ts_const + sizeof(TsDev));
-  TsCoef* d_co_all = reinterpret_cast<TsCoef*>(ctx->ts_const + off_co);
+  TsShellCoef* d_co = reinterpret_cast<TsShellCoef*>(ctx->ts_const + off_co);
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(d_hc, &hc, sizeof(TsDev), cudaMemcpyHostToDevice, st));
   RG_CUDA_TRY(ctx, cudaMemsetAsync(d_nonconv, 0, sizeof(int), st));
   const int nblk = 148 * 8;
@@ -637,8 +685,8 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double Mh2 = rtom(p, R0) * p->Hubble_h * p->Hubble_h;
   const double ftpr3 = (4.0 / 3.0) * M_PI * std::pow(R0, 3.0) / pixel_volume;
 
-  auto finish = [&](bool homog) -> int {
-    if ((rc = reduce_partials(ctx, partials, nblk, TS_NSUM, ctx->d_sums, st))) return rc;
+  auto finish = [&](bool homog, int nblocks) -> int {
+    if ((rc = reduce_partials(ctx, partials, nblocks, TS_NSUM, ctx->d_sums, st))) return rc;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * TS_NSUM, cudaMemcpyDeviceToHost, st));
     int nonconv = 0;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(&nonconv, d_nonconv, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -677,11 +725,11 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     const float xe0 = (float)xion_RECFAST(ctx->tables, (float)zp);
     const float TK0 = (float)T_RECFAST(ctx->tables, (float)zp);
     prof_begin(ctx, "ts_homog", st);
-    k_ts_homog<<<nblk, 256, 0, st>>>(d_hc, (float)zp, xe0, TK0, cT_approx((float)zp), N, g->deltax, g->x_e_box_prev,
+    k_ts_homog<<<nblk, 256, 0, st>>>(d_hc, xe0, TK0, cT_approx((float)zp), N, g->deltax, g->x_e_box_prev,
                                       g->x_e_box, g->Tk_box, g->TS_box, partials, d_nonconv);
     prof_end(ctx, 28.0 * n3, st);
     RG_CUDA_TRY(ctx, cudaGetLastError());
-    return finish(true);
+    return finish(true, nblk);
   }
 
   // inhomogeneous branch
@@ -693,7 +741,10 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double prev_redshift = s->snapshot == 0 ? s->ZZ[s->snapshot] : s->ZZ[s->snapshot - 1];
   const size_t nc = (size_t)(N / 2 + 1) * N * N;
   const size_t npad = (size_t)N * N * 2 * (N / 2 + 1);
-  if ((rc = ensure_mem(ctx, &ctx->ts_acc, &ctx->ts_acc_elems, 4 * n3))) return rc;
+  TsZev zv;
+  std::memset(&zv, 0, sizeof(zv));
+  for (int m = 0; m < x_int_NXHII; ++m) zv.X[m] = ctx->tables.x_int_XHII[m];
+  for (int k = 0; k < 4; ++k) zv.inv_scale[k] = 1.0;
 
   if (!no_light) {
     if (!s->stored_fcoll && s->snapshot > 0)
@@ -718,8 +769,8 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     }
     const int nused = std::max(1, (int)used.size());
     if ((rc = ensure_mem(ctx, &ctx->spec, &ctx->spec_elems, nc * 2 * nused))) return rc;
-    const int kb = std::min(TS_KB, nS);
-    if ((rc = ensure_mem(ctx, &ctx->work, &ctx->work_elems, nc * 2 * kb))) return rc;
+    // every shell's filtered grids stay in HBM until the fused z pass (2 nS spectra)
+    if ((rc = ensure_mem(ctx, &ctx->work, &ctx->work_elems, nc * 2 * nS))) return rc;
     // source grid `which` (0 sfr, 1 xray) of source k, on the device
     const rg_grids* sg = src_host ? src_host : g;
     auto src_grid = [&](int k, int which) -> const float* {
@@ -782,32 +833,32 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       cs[r] = convS * opzf2 * (1 + sh.zpp[r]) * tb.sum_lyn[r] * a;
       maxk[3] = std::max(maxk[3], std::fabs(cs[r]));
     }
-    // FP32 within a batch: scale each sum by a power of two that brings its largest
+    // FP32 sums over the shells: scale each sum by a power of two that brings its largest
     // per-shell coefficient near 1 (values of order 1e-30 would lose range in float)
     double scale[4];
-    for (int k = 0; k < 4; ++k) scale[k] = pow2_scale(maxk[k]);
-    TsCoef* d_co = d_co_all;
-    const int nbatch = (nS + kb - 1) / kb;
-    std::vector<TsCoef> hco(nbatch);
-    for (int bi = 0; bi < nbatch; ++bi) {
-      const int r0 = bi * kb, cnt = std::min(kb, nS - r0);
-      TsCoef& co = hco[bi];
-      std::memset(&co, 0, sizeof(co));
-      co.nr = cnt;
-      co.first = bi == 0;
-      for (int m = 0; m < x_int_NXHII; ++m) co.X[m] = X[m];
-      for (int k = 0; k < 4; ++k) co.inv_scale[k] = 1.0 / scale[k];
+    for (int k = 0; k < 4; ++k) {
+      scale[k] = pow2_scale(maxk[k]);
+      zv.inv_scale[k] = 1.0 / scale[k];
+    }
+    std::vector<TsShellCoef> hco(nS + 1);
+    std::memset(hco.data(), 0, sizeof(TsShellCoef) * hco.size());
+    for (int r = 0; r < nS; ++r) {
+      for (int kind = 0; kind < 3; ++kind)
+        for (int m = 0; m < x_int_NXHII; ++m) {
+          hco[r].P[kind][m] = (float)(Pd[((size_t)r * 3 + kind) * x_int_NXHII + m] * scale[kind]);
+          hco[r].Q[kind][m] = (float)(Qd[((size_t)r * 3 + kind) * x_int_NXHII + m] * scale[kind]);
+        }
+      hco[r].cstar = (float)(cs[r] * scale[3]);
+    }
+    RG_CUDA_TRY(ctx, cudaMemcpyAsync(d_co, hco.data(), sizeof(TsShellCoef) * (nS + 1), cudaMemcpyHostToDevice, st));
+    // x and y passes in batches of TS_KB shells into work[r][g]
+    for (int r0 = 0; r0 < nS; r0 += TS_KB) {
+      const int cnt = std::min(TS_KB, nS - r0);
       TsBatch bt;
       std::memset(&bt, 0, sizeof(bt));
       bt.nr = cnt;
       for (int j = 0; j < cnt; ++j) {
         const int r = r0 + j;
-        for (int kind = 0; kind < 3; ++kind)
-          for (int m = 0; m < x_int_NXHII; ++m) {
-            co.P[j][kind][m] = (float)(Pd[((size_t)r * 3 + kind) * x_int_NXHII + m] * scale[kind]);
-            co.Q[j][kind][m] = (float)(Qd[((size_t)r * 3 + kind) * x_int_NXHII + m] * scale[kind]);
-          }
-        co.cstar[j] = (float)(cs[r] * scale[3]);
         int nk = 0;
         for (int k = 0; k < sh.nsrc; ++k) {
           const float c = sh.coef[(size_t)r * sh.nsrc + k];
@@ -821,31 +872,33 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
         bt.filtered[j] = r > 0;  // no filter on the first shell (ComputeTs.c:529)
         bt.wrow[j] = r;
       }
-      RG_CUDA_TRY(ctx, cudaMemcpyAsync(d_co + bi, &co, sizeof(TsCoef), cudaMemcpyHostToDevice, st));
-      if ((rc = ts_batch(ctx, N, ctx->spec, ctx->work, nc, bt, ctx->wtab, n2max + 1, d_co + bi, g->x_e_box_prev,
-                         ctx->ts_acc, st)))
+      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, st)))
         return rc;
     }
-    RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // hco outlives the copies
+    zv.nS = nS;
+    if ((rc = ensure_mem(ctx, &ctx->ts_sums, &ctx->ts_sums_elems, n3))) return rc;
+    if ((rc = ts_zsum(ctx, N, ctx->work, nc, d_co, zv, g->x_e_box_prev, ctx->ts_sums, st))) return rc;
+    RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // hco outlives the copy
   }
 
   TsEvolve e;
-  e.zp_f = (float)zp;
   e.zp = zp;
   e.dzp = zp - prev_redshift;
   e.dt_dzp = pf.dt_dzp;
+  e.heat_conv = pf.dt_dzp * 2.0 / 3.0 / BOLTZMANN;
   e.growth = pf.growth_factor_zp;
   e.dgrowth = pf.dgrowth_factor_dzp;
   e.const_zp = pf.const_zp_prefactor_GAL;
   // Conversion_factor (XRayHeatingFunctions.c:1331-1332)
   e.conv_star = (SPEED_OF_LIGHT / (4. * M_PI)) / (PROTONMASS / SOLAR_MASS);
   e.no_light = no_light;
+  const double4 inv = make_double4(zv.inv_scale[0], zv.inv_scale[1], zv.inv_scale[2], zv.inv_scale[3]);
   prof_begin(ctx, "ts_evolve", st);
-  k_ts_evolve<<<nblk, 256, 0, st>>>(d_hc, e, N, ctx->ts_acc, g->deltax, g->x_e_box_prev, g->x_e_box, g->Tk_box,
-                                     g->TS_box, partials, d_nonconv);
-  prof_end(ctx, (double)n3 * (32 + 4 + 4 + 4 + 4 + 4 + 4 + 4), st);
+  k_ts_evolve<<<nblk, 256, 0, st>>>(d_hc, e, inv, N, no_light ? nullptr : ctx->ts_sums, g->deltax, g->x_e_box_prev,
+                                     g->x_e_box, g->Tk_box, g->TS_box, partials, d_nonconv);
+  prof_end(ctx, (double)n3 * (16 + 4 + 4 + 4 + 4 + 4 + 4 + 4), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
-  return finish(false);
+  return finish(false, nblk);
 }
 
 }  // namespace rg

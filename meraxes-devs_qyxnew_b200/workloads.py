@@ -152,6 +152,8 @@ CONFIGS = {
     "c3_128": GridConfig("c3_128", 128, 128.0, 15.0, spin_temp=1, seed=1812),
     # full step at 512^3, 500 Mpc/h, z=8, R0 = 0.62*L (about 60 radii), then Ts and delta_T
     "c4_512": GridConfig("c4_512", 512, 500.0, 8.0, r_bubble_max=1000.0, spin_temp=1, seed=1813),
+    # the same step at 256^3 (250 Mpc/h): the small case for kernel captures (inputs still > L2)
+    "c4_256": GridConfig("c4_256", 256, 250.0, 8.0, r_bubble_max=1000.0, spin_temp=1, seed=1813),
 }
 
 
