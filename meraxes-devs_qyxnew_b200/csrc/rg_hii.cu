@@ -54,7 +54,7 @@ __global__ void k_window_table(float* wtab, int n2max, const double* __restrict_
 // Radius r uses window row wrows + r * wpitch, or none when r == unfiltered.
 
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<N>::BX))
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, (x_pass_minb<N>()))
     k_hii_x(const cf* __restrict__ spec, size_t stride, int ng, cf* __restrict__ work, int nr,
             const float* __restrict__ wrows, int wpitch, int unfiltered, const cf* __restrict__ g_tw) {
   constexpr int T = Cfg<N>::T, B = Cfg<N>::BX, V = Cfg<N>::V;

@@ -70,6 +70,14 @@ struct Cfg {
   static constexpr int RT_PITCH = N + 1;  // real row pitch (floats) in zfront
 };
 
+// minimum resident blocks of the windowed inverse x passes: with radix-8 plans two blocks of 512
+// threads (at most 64 registers); otherwise the general cap
+template <int N>
+constexpr int x_pass_minb() {
+  constexpr int nth = Cfg<N>::T * Cfg<N>::BX;
+  return (Cfg<N>::V <= 8 && nth >= 512) ? 2 : RG_MINB(nth);
+}
+
 // exchange-buffer index of position p of line b when threads walk positions (one pad slot
 // every 16 positions breaks the stride-R write pattern of the first stages)
 template <int N>

@@ -199,7 +199,7 @@ struct TsBatch {
 };
 
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<N>::BX))
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, (x_pass_minb<N>()))
     k_ts_x(const cf* __restrict__ spec, size_t stride, cf* __restrict__ work, TsBatch bt,
            const float* __restrict__ wtab, int wpitch, const cf* __restrict__ g_tw) {
   constexpr int T = Cfg<N>::T, B = Cfg<N>::BX, V = Cfg<N>::V;
