@@ -195,10 +195,13 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<
   constexpr int IT = ROWS * N / NTH;   // cells per thread
   constexpr int W = (IT + 31) / 32;    // bit words per thread
   static_assert(ROWS * N % NTH == 0, "whole rows per block");
-  extern __shared__ cf smem[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // 16-byte aligned for cp.async
+  cf* smem = reinterpret_cast<cf*>(smem_raw);
   cf* s_tw = smem;
   cf* xbuf = smem + N;
   float* rt = reinterpret_cast<float*>(xbuf + line_buf<N, Q>());
+  // two shared tiles: grid u + 1 is copied while grid u is transformed
+  cf* tiles = reinterpret_cast<cf*>(rt + round_up(NG * ROWS * RP, 4));
   const int x = blockIdx.y, y0 = blockIdx.x * ROWS;
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const size_t nwords = (size_t)gridDim.x * gridDim.y * W * NTH;
@@ -231,9 +234,30 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<
 #pragma unroll
   for (int k = 0; k < (FINAL ? HII_NSUM : 1); ++k) acc[k] = 0.0;
 
+  const int nunits = bt.nr * NG;   // (radius, grid) pairs, unit u = r * NG + g
+  ztile_issue<N, Q>(tiles, work, x, y0, NTH);
+  cp_async_commit();
+  const int q = threadIdx.x % Q, tq = threadIdx.x / Q;
   for (int r = 0; r < bt.nr; ++r) {
     __syncthreads();  // rt of the previous radius is consumed
-    zfront<N, NG>(work + (size_t)r * NG * stride, stride, s_tw, xbuf, rt, x, y0);
+#pragma unroll 1
+    for (int g = 0; g < NG; ++g) {
+      const int u = r * NG + g;
+      if (u + 1 < nunits) ztile_issue<N, Q>(tiles + ((u + 1) & 1) * ztile_elems<N>(), work + (size_t)(u + 1) * stride, x, y0, NTH);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();  // unit u's tile is complete for every thread
+      const cf* tile = tiles + (u & 1) * ztile_elems<N>();
+      float* r0 = rt + (size_t)(g * ROWS + 2 * q) * RP;
+      line_fft<N, true>(
+          tq, xbuf, s_tw, [&](int p, int) { return ztile_c2r_input<N, Q>(tile, q, p); },
+          [&](int p) { return line_addr<N, Q>(p, q); },
+          [&](int p, cf v) {
+            r0[p] = v.x;
+            r0[RP + p] = v.y;
+          });
+      __syncthreads();  // the tile is consumed before unit u + 2 refills it; rt row is written
+    }
     const bool last = FINAL && r == bt.nr - 1;
     const double pref = bt.fcoll_pref[r];
 #pragma unroll
@@ -435,7 +459,8 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
-  const size_t sm = zfront_smem_bytes<N>(NG);
+  const size_t sm = sizeof(cf) * (N + (size_t)line_buf<N, C::QZ>()) +
+                    sizeof(float) * (size_t)round_up(NG * 2 * C::QZ * C::RT_PITCH, 4) + sizeof(cf) * 2 * ztile_elems<N>();
   RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL>, sm));
   const dim3 grid(N / (2 * C::QZ), N);
   // algorithmic bytes: the Hermitian halves of NG grids per radius, z_at_ionization on the

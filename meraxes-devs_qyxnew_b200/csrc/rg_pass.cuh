@@ -228,6 +228,46 @@ __device__ __forceinline__ void zfront(const cf* __restrict__ work, size_t strid
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// asynchronous global -> shared copies (cp.async, 16 bytes per instruction); the copies of a
+// commit group complete in order, wait<n> leaves at most n groups in flight
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int n>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
+}
+
+// the Hermitian halves of rows [y0, y0 + 2Q) of plane x of one grid as a shared tile
+// tile[k][j] = g[k][x][y0 + j], k <= N/2, j < 2Q, copied by the whole block
+template <int N, int Q>
+__device__ __forceinline__ void ztile_issue(cf* tile, const cf* __restrict__ g, int x, int y0, int nth) {
+  constexpr int NZ = N / 2 + 1;
+  for (int c = threadIdx.x; c < NZ * Q; c += nth) {
+    const int k = c / Q, j = 2 * (c % Q);
+    cp_async16(tile + k * 2 * Q + j, g + ((size_t)k * N + x) * N + y0 + j);
+  }
+}
+
+// build_c2r_input from a shared tile (row pair q)
+template <int N, int Q>
+__device__ __forceinline__ cf ztile_c2r_input(const cf* tile, int q, int p) {
+  const int k = p <= N / 2 ? p : N - p;
+  const float4 ab = *reinterpret_cast<const float4*>(tile + k * 2 * Q + 2 * q);
+  if (p == 0 || p == N / 2) return cf{ab.x, ab.z};
+  if (p < N / 2) return cf{ab.x - ab.w, ab.y + ab.z};
+  return cf{ab.x + ab.w, ab.z - ab.y};
+}
+
+template <int N>
+constexpr size_t ztile_elems() {
+  return (size_t)(N / 2 + 1) * 2 * Cfg<N>::QZ;
+}
+
 // c2r of one spectrum into a padded real grid (tests)
 template <int N>
 __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<N>::QZ))
