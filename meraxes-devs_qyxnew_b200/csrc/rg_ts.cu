@@ -343,17 +343,38 @@ struct TsZ {
   static constexpr int Q = pow2_div(N, cmax(256 / T, 4));   // rows per block
   static constexpr int NTH = T * Q;
   static constexpr int MINB = NTH >= 512 ? 1 : 512 / NTH;   // 2 blocks of 256: at most 128 registers
-  static constexpr size_t smem() { return sizeof(cf) * (N + (size_t)line_buf_r0<N, R0, Q>()); }
+  static constexpr size_t tile_elems() { return (size_t)2 * (N / 2 + 1) * Q; }   // two shells' rows
+  static constexpr size_t smem() {
+    return sizeof(cf) * (N + (size_t)line_buf_r0<N, R0, Q>() + 2 * tile_elems());
+  }
 };
 
-// complex line of rows (x, y) of two shells' Hermitian halves a, b (b may be null)
-template <int N>
-__device__ __forceinline__ cf pair_c2r_input(const cf* __restrict__ a, const cf* __restrict__ b, size_t col, int p) {
+// the Hermitian halves of rows [y0, y0 + Q) of plane x of two shells' grids a, b (b may be null:
+// zeros) as a shared tile tile[s][k][j] = (s ? b : a)[k][x][y0 + j], copied by the whole block
+template <int N, int Q>
+__device__ __forceinline__ void ts_tile_issue(cf* tile, const cf* __restrict__ a, const cf* __restrict__ b, int x,
+                                              int y0, int nth) {
+  constexpr int NZ = N / 2 + 1, C = NZ * Q / 2;   // 16-byte chunks per shell
+  for (int c = threadIdx.x; c < 2 * C; c += nth) {
+    const int s = c / C, cc = c % C;
+    const int k = cc / (Q / 2), j = 2 * (cc % (Q / 2));
+    cf* dst = tile + ((size_t)s * NZ + k) * Q + j;
+    const cf* g = s ? b : a;
+    if (g) {
+      cp_async16(dst, g + ((size_t)k * N + x) * N + y0 + j);
+    } else {
+      dst[0] = cf{0.f, 0.f};
+      dst[1] = cf{0.f, 0.f};
+    }
+  }
+}
+
+// complex line of row q of the two shells in a tile (shell a real part, shell b imaginary part)
+template <int N, int Q>
+__device__ __forceinline__ cf ts_tile_input(const cf* tile, int q, int p) {
+  constexpr int NZ = N / 2 + 1;
   const int k = p <= N / 2 ? p : N - p;
-  const size_t o = col + (size_t)k * N * N;
-  const float2 A = __ldg(reinterpret_cast<const float2*>(a + o));
-  float2 B = make_float2(0.f, 0.f);
-  if (b) B = __ldg(reinterpret_cast<const float2*>(b + o));
+  const cf A = tile[k * Q + q], B = tile[(NZ + k) * Q + q];
   if (p == 0 || p == N / 2) return cf{A.x, B.x};
   if (p < N / 2) return cf{A.x - B.y, A.y + B.x};
   return cf{A.x + B.y, B.x - A.y};
@@ -368,9 +389,11 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
   using PL = typename Z::PL;
   constexpr int Q = Z::Q, V = Z::V;
   constexpr int PADW = 2 * (N / 2 + 1);
-  extern __shared__ cf smem[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];  // 16-byte aligned for cp.async
+  cf* smem = reinterpret_cast<cf*>(smem_raw);
   cf* s_tw = smem;
   cf* xbuf = smem + N;
+  cf* tiles = xbuf + line_buf_r0<N, Z::R0, Q>();
   __shared__ TsShellCoef sc[2];
   const int x = blockIdx.y, y = blockIdx.x * Q + threadIdx.x % Q;
   const int t = threadIdx.x / Q;
@@ -405,32 +428,44 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
 #pragma unroll
   for (int sl = 0; sl < V; ++sl) a_heat[sl] = a_ion[sl] = a_lya[sl] = a_star[sl] = 0.f;
   auto addr = [&](int p) { return line_addr_r0<Z::R0, Q>(p, threadIdx.x % Q); };
-  for (int r = 0; r < zv.nS; r += 2) {
-    const bool two = r + 1 < zv.nS;
-    __syncthreads();  // readers of the previous pair's coefficients are done
-    {
+  // units u = 2 (r / 2) + g: the pair of shells (r, r + 1), grid g (0 sfr, 1 X-ray); the tile of
+  // unit u + 1 is copied while unit u is transformed
+  const int y0 = blockIdx.x * Q, q = threadIdx.x % Q;
+  auto unit_src = [&](int u, int which) -> const cf* {
+    const int r = 2 * (u >> 1) + which, g = u & 1;
+    return r < zv.nS ? work + ((size_t)r * 2 + g) * stride : nullptr;
+  };
+  const int nunits = 2 * ((zv.nS + 1) / 2);
+  if (nunits > 0) ts_tile_issue<N, Q>(tiles, unit_src(0, 0), unit_src(0, 1), x, y0, Z::NTH);
+  cp_async_commit();
+  for (int u = 0; u < nunits; ++u) {
+    const int r = 2 * (u >> 1);
+    if ((u & 1) == 0) {
+      __syncthreads();  // readers of the previous pair's coefficients are done
+      const bool two = r + 1 < zv.nS;
       const int* src = reinterpret_cast<const int*>(gco + r);
       int* dst = reinterpret_cast<int*>(sc);
       const int nwords = (two ? 2 : 1) * (int)(sizeof(TsShellCoef) / sizeof(int));
       for (int i = threadIdx.x; i < (int)(2 * sizeof(TsShellCoef) / sizeof(int)); i += Z::NTH)
         dst[i] = i < nwords ? src[i] : 0;
     }
-    __syncthreads();
-    // sfr: stellar Lyman-alpha sum, SFR clamped at 0 (ComputeTs.c:700)
-    {
-      const cf* ga = work + ((size_t)r * 2 + 0) * stride;
-      const cf* gb = two ? work + ((size_t)(r + 1) * 2 + 0) * stride : nullptr;
+    if (u + 1 < nunits)
+      ts_tile_issue<N, Q>(tiles + ((u + 1) & 1) * Z::tile_elems(), unit_src(u + 1, 0), unit_src(u + 1, 1), x, y0,
+                          Z::NTH);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();  // unit u's tile (and the pair's coefficients) are visible to every thread
+    const cf* tile = tiles + (u & 1) * Z::tile_elems();
+    if ((u & 1) == 0) {
+      // sfr: stellar Lyman-alpha sum, SFR clamped at 0 (ComputeTs.c:700)
       const float c0 = sc[0].cstar, c1 = sc[1].cstar;
       line_fft_p<PL, true>(
-          t, xbuf, s_tw, [&](int p, int) { return pair_c2r_input<N>(ga, gb, row, p); }, addr,
+          t, xbuf, s_tw, [&](int p, int) { return ts_tile_input<N, Q>(tile, q, p); }, addr,
           [&](int, cf v, int sl) { a_star[sl] += fmaxf(v.x, 0.f) * c0 + fmaxf(v.y, 0.f) * c1; });
-    }
-    // X-ray: heating, ionisation and Lyman-alpha integrands, not clamped
-    {
-      const cf* ga = work + ((size_t)r * 2 + 1) * stride;
-      const cf* gb = two ? work + ((size_t)(r + 1) * 2 + 1) * stride : nullptr;
+    } else {
+      // X-ray: heating, ionisation and Lyman-alpha integrands, not clamped
       line_fft_p<PL, true>(
-          t, xbuf, s_tw, [&](int p, int) { return pair_c2r_input<N>(ga, gb, row, p); }, addr,
+          t, xbuf, s_tw, [&](int p, int) { return ts_tile_input<N, Q>(tile, q, p); }, addr,
           [&](int, cf v, int sl) {
             const int lo = (int)((lopack >> (4 * sl)) & 15u);
             const float d = dxe[sl];
@@ -439,6 +474,7 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
             a_lya[sl] += v.x * fmaf(d, sc[0].Q[2][lo], sc[0].P[2][lo]) + v.y * fmaf(d, sc[1].Q[2][lo], sc[1].P[2][lo]);
           });
     }
+    __syncthreads();  // the tile is consumed before unit u + 2 refills it
   }
 #pragma unroll
   for (int sl = 0; sl < V; ++sl)
