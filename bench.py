@@ -168,9 +168,10 @@ def traffic_from_profiles(kernel: str, cfg_name: str):
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return None
+    pat = re.compile(r"traffic_bytes_per_launch\[" + re.escape(kernel) + "@" + re.escape(cfg_name) + r"\]:\s*([0-9.eE+]+)")
     for f in sorted(os.listdir(pdir)):
-        if kernel in f and cfg_name in f and f.endswith(".md"):
-            m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(os.path.join(pdir, f)).read())
+        if f.endswith(".md"):
+            m = pat.search(open(os.path.join(pdir, f)).read())
             if m:
                 return float(m.group(1))
     return None
