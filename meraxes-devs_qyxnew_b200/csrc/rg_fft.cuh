@@ -199,6 +199,20 @@ constexpr int plan_product() {
   return p;
 }
 
+// Twiddles are kept per stage: stage s >= 1 owns entries [tw_offset(s), tw_offset(s) + NS (R - 1))
+// with entry jm (R - 1) + (r - 1) = e^{-2 pi i r jm / (NS R)}, so threads with consecutive jm
+// read consecutive words (a table indexed by r jm N / (NS R) puts them on a few banks).  The
+// stages together hold N - R_0 entries.
+template <class PL>
+__host__ __device__ constexpr int tw_offset(int s) {
+  int off = 0, ns = PL::R[0];
+  for (int i = 1; i < s; ++i) {
+    off += ns * (PL::R[i] - 1);
+    ns *= PL::R[i];
+  }
+  return off;
+}
+
 // Stage-0 input position of register slot `slot` (0 <= slot < N/T) of thread t.
 template <class PL>
 __device__ __forceinline__ int stage0_pos(int t, int slot) {
@@ -224,9 +238,10 @@ __device__ __forceinline__ void stage_compute(cf* v, int t, const cf* __restrict
     for (int r = 0; r < R; ++r) v[k * R + r] = load(j + r * (N / R), k * R + r);
     if constexpr (NS > 1) {
       const int jm = j % NS;
+      constexpr int OFF = tw_offset<PL>(s);
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        cf w = tw[(r * jm * (N / (NS * R))) % N];
+        cf w = tw[OFF + jm * (R - 1) + (r - 1)];
         if (INV) w.y = -w.y;
         v[k * R + r] = cmul(v[k * R + r], w);
       }
@@ -301,10 +316,30 @@ __device__ __forceinline__ int stage0_pos(int t, int slot) {
   return stage0_pos<Plan<N>>(t, slot);
 }
 
-// Copy the N-entry twiddle table into shared memory (caller syncs).
+// Fill the per-stage twiddle tables of plan PL in shared memory from the N-entry table
+// g_tw[k] = e^{-2 pi i k / N} (caller syncs).
+template <class PL, int s>
+__device__ __forceinline__ void load_twiddle_stages(cf* s_tw, const cf* __restrict__ g_tw) {
+  if constexpr (s < PL::S) {
+    constexpr int N = PL::NN;
+    constexpr int R = PL::R[s];
+    constexpr int NS = StageNS<PL, s>::value;
+    constexpr int OFF = tw_offset<PL>(s);
+    for (int i = threadIdx.x; i < NS * (R - 1); i += blockDim.x) {
+      const int jm = i / (R - 1), r = i % (R - 1) + 1;
+      s_tw[OFF + i] = g_tw[(r * jm * (N / (NS * R))) % N];
+    }
+    load_twiddle_stages<PL, s + 1>(s_tw, g_tw);
+  }
+}
+template <class PL>
+__device__ __forceinline__ void load_twiddles_p(cf* s_tw, const cf* __restrict__ g_tw) {
+  load_twiddle_stages<PL, 1>(s_tw, g_tw);
+}
+// the default plan's tables (N entries of shared memory always suffice)
 template <int N>
 __device__ __forceinline__ void load_twiddles(cf* s_tw, const cf* __restrict__ g_tw) {
-  for (int i = threadIdx.x; i < N; i += blockDim.x) s_tw[i] = g_tw[i];
+  load_twiddles_p<Plan<N>>(s_tw, g_tw);
 }
 
 }  // namespace rg

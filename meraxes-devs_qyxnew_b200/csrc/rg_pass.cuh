@@ -80,8 +80,12 @@ constexpr int x_pass_minb() {
 
 // exchange-buffer index of position p of line b when threads walk positions (one pad slot
 // every 16 positions breaks the stride-R write pattern of the first stages)
+// For 192, 384 and 512 points an XOR of position bits 3-6 into bits 0-3 (a bijection within
+// each 16-position group) spreads every exchange of the plan over all banks; for the other sizes
+// the pad slot does.
 template <int N>
 __device__ __forceinline__ int pos_addr(int b, int p) {
+  if constexpr (N == 192 || N == 384 || N == 512) return b * Cfg<N>::PITCH_P + (p ^ ((p >> 3) & 15));
   return b * Cfg<N>::PITCH_P + p + (p >> 4);
 }
 // exchange-buffer index when threads walk lines (B consecutive lines per position).  With

@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
   __shared__ TsShellCoef sc[2];
   const int x = blockIdx.y, y = blockIdx.x * Q + threadIdx.x % Q;
   const int t = threadIdx.x / Q;
-  load_twiddles<N>(s_tw, g_tw);
+  load_twiddles_p<PL>(s_tw, g_tw);
   const size_t row = (size_t)x * N + y;
   // this thread's cells: z = last_pos(t, s); x_e interpolation node and offset
   // (ComputeTs.c:1198-1209)
