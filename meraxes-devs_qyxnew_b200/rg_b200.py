@@ -162,6 +162,16 @@ def make_params(n: int, box: float, **kw) -> rg_params:
     return p
 
 
+def radius_schedule(p: rg_params, redshift: float, max_r: int = 4096):
+    """The filter radii of find_HII_bubbles at this redshift (host computation)."""
+    import numpy as np
+    radii = np.zeros(max_r)
+    n = C.c_int()
+    check(None, load().rg_radius_schedule(C.byref(p), redshift, radii.ctypes.data_as(C.POINTER(C.c_double)), max_r,
+                                          C.byref(n)))
+    return radii[: n.value].copy()
+
+
 def ts_tables(p: rg_params, zz, snap: int, n_hist: int, x_e_ave: float, collapse_fraction: float,
               stored_fcoll=None, with_freq: bool = True):
     """The host coefficient engine of the spin-temperature step (no device work): returns

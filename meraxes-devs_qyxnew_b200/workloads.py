@@ -210,3 +210,38 @@ def make_ts_inputs(src: SourceGrids, zz: np.ndarray, snap: int, n_hist: int, see
         sf[snap - 1] = fcoll_prev
     return TsInputs(x_e_box_prev=to_padded(xe), Tk_box=tk, sfr_histories=sfr_h, xray_histories=xr_h,
                     stored_fcoll=sf)
+
+
+# The batched workload: 48 independent snapshots spanning z = 16 -> 6 over boxes of uneven size
+# (64^3, 96^3, 128^3, 192^3, 12 each, L = N Mpc/h).  The sources are the generators above; the
+# ionising efficiency per redshift is interpolated (in log) from a calibration of the 64^3 box
+# against the CPU oracle so that mean xH runs linearly from 0.99 at z = 16 to 0.1 at z = 6.
+BATCH_EFFICIENCY = [(16.0, 563.0), (14.0, 11913.0), (12.0, 19338.0), (10.0, 24313.0), (8.0, 28013.0),
+                    (6.0, 29729.0)]
+BATCH_SIZES = (64, 96, 128, 192)
+BATCH_UNITS = 48
+
+
+def batch_efficiency(z: float) -> float:
+    zs = [a for a, _ in BATCH_EFFICIENCY][::-1]
+    ls = [math.log(b) for _, b in BATCH_EFFICIENCY][::-1]
+    return math.exp(float(np.interp(z, zs, ls)))
+
+
+@dataclasses.dataclass
+class BatchUnit:
+    index: int
+    n: int
+    box: float
+    z: float
+    efficiency: float
+    seed: int
+
+
+def batch_units(count: int = BATCH_UNITS) -> list[BatchUnit]:
+    out = []
+    for i in range(count):
+        z = 16.0 - 10.0 * i / (count - 1)
+        n = BATCH_SIZES[i % len(BATCH_SIZES)]
+        out.append(BatchUnit(i, n, float(n), z, batch_efficiency(z), 1811 + i))
+    return out

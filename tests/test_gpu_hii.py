@@ -27,7 +27,7 @@ def _recfast():
 
 
 @pytest.mark.parametrize("n,box", [(8, 8.0), (16, 20.0), (24, 24.0), (32, 32.0), (48, 48.0), (64, 64.0),
-                                   (96, 96.0), (128, 100.0)])
+                                   (96, 96.0), (128, 100.0), (256, 250.0)])
 @pytest.mark.parametrize("ftype", [-1, 0, 1, 2])
 def test_filter_roundtrip_matches_fp64(n, box, ftype):
     import torch
@@ -124,14 +124,36 @@ def test_find_hii_bubbles_config_efficiency():
     assert out.volume_weighted_global_xH > 0.99
 
 
+def compare_modes(n, box, z, seed, eff=4000.0):
+    """The fused mode (radius batches, windowed inverse passes, two-for-one c2r) against the plain
+    mode (one FFT chain per grid per radius, every reference grid).  Both are FP32 evaluations of
+    the same sums; where the compiler contracts them differently the rounding differs, so:
+    ionised flags differ in <= 0.01% of cells, J_21 and the temperatures agree to 1e-5 relative L2,
+    the box averages to 1e-5."""
+    src = wl.make_sources(n, box, seed=seed)
+    a, oa, _ = run_gpu_hii(n, box, z, src, eff, mode=rg.RG_MODE_FUSED)
+    b, ob, _ = run_gpu_hii(n, box, z, src, eff, mode=rg.RG_MODE_PLAIN)
+    ia, ib = a.get("xH") < ro.REL_TOL, b.get("xH") < ro.REL_TOL
+    assert (ia != ib).mean() <= 1e-4
+    same = ia == ib
+    assert np.array_equal(a.get("z_at_ionization")[same], b.get("z_at_ionization")[same])
+    for k in ("J_21_at_ionization", "temp_kinetic_all_gas"):
+        assert rel_l2(a.get(k)[same], b.get(k)[same]) <= 1e-5, k
+    assert np.max(np.abs(a.get("xH")[same] - b.get("xH")[same])) <= 1e-4
+    da, db = oa.as_dict(), ob.as_dict()
+    for k in da:
+        assert da[k] == pytest.approx(db[k], rel=1e-5, abs=1e-12), k
+    return oa
+
+
 def test_plain_mode_matches_fused():
-    n, box, z = 64, 64.0, 8.0
-    src = wl.make_sources(n, box, seed=5)
-    a, oa, _ = run_gpu_hii(n, box, z, src, 4000.0, mode=rg.RG_MODE_FUSED)
-    b, ob, _ = run_gpu_hii(n, box, z, src, 4000.0, mode=rg.RG_MODE_PLAIN)
-    for k in ("xH", "z_at_ionization", "J_21_at_ionization", "temp_kinetic_all_gas"):
-        assert np.array_equal(a.get(k), b.get(k)), k
-    assert oa.as_dict() == ob.as_dict()
+    compare_modes(64, 64.0, 8.0, 5)
+
+
+@pytest.mark.parametrize("n,box", [(256, 250.0), (512, 500.0)])
+def test_plain_mode_matches_fused_large(n, box):
+    oa = compare_modes(n, box, 8.0, 6)
+    assert 0.0 < oa.volume_weighted_global_xH < 1.0
 
 
 def test_host_entry_point_matches_device():
