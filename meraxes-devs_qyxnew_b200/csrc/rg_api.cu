@@ -286,6 +286,11 @@ int rg_create(int device, int grid_dim, rg_context** out) {
     return RG_ECUDA;
   }
   ctx->stream = ctx->own_stream;
+  if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      ctx->num_sms < 1) {
+    rg_destroy(ctx);
+    return RG_ECUDA;
+  }
   if (cudaMallocHost((void**)&ctx->h_sums, sizeof(double) * 64) != cudaSuccess ||
       cudaMalloc((void**)&ctx->d_sums, sizeof(double) * 64) != cudaSuccess) {
     rg_destroy(ctx);
@@ -311,6 +316,7 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->ts_stage) cudaFree(ctx->ts_stage);
   if (ctx->ts_const) cudaFree(ctx->ts_const);
   if (ctx->ts_sums) cudaFree(ctx->ts_sums);
+  if (ctx->xy_ctrl) cudaFree(ctx->xy_ctrl);
   for (void* p : ctx->owned) cudaFree(p);
   prof_resolve(ctx);
   for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);

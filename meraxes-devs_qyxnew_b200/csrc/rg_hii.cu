@@ -21,6 +21,7 @@
 
 #include "rg_internal.h"
 #include "rg_pass.cuh"
+#include "rg_xyf.cuh"
 
 namespace rg {
 
@@ -429,15 +430,38 @@ int launch_forward(rg_context* ctx, const float* const* d_real, int ng, cf* spec
   return RG_OK;
 }
 
-// inverse x (window, batch of nr radii) and y passes
+// the batch of the fused x/y pass: grid g of spec windowed for radius r into work (r ng + g)
+struct HiiXOp {
+  const cf* spec;
+  size_t stride;
+  int ng;
+  cf* work;
+  const float* wrows;
+  int wpitch;
+  int unfiltered;
+  __device__ int grids() const { return ng; }
+  __device__ int nsrc(int) const { return 1; }
+  __device__ const cf* src(int, int g, int) const { return spec + g * stride; }
+  __device__ float coef(int, int) const { return 1.f; }
+  __device__ bool filtered(int r) const { return r != unfiltered; }
+  __device__ const float* wrow(int r) const { return wrows + (size_t)r * wpitch; }
+  __device__ cf* out(int r, int g) const { return work + ((size_t)r * ng + g) * stride; }
+};
+
+// inverse x (window, batch of nr radii) and y passes: one fused kernel, or (plain mode) the two
+// passes as separate kernels
 template <int N>
 int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, cf* work, size_t stride, int nr, const float* wrows,
                       int wpitch, int unfiltered, cudaStream_t st) {
+  using C = Cfg<N>;
+  const double nzc = (double)C::NZ * N * N;
+  if (ctx->mode == RG_MODE_FUSED) {
+    const HiiXOp op{spec, stride, ng, work, wrows, wpitch, unfiltered};
+    return launch_xy_fused<N>(ctx, op, nr, "inv_xy_c2c_window", ng * 8.0 * nzc * (1 + nr), st);
+  }
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
-  using C = Cfg<N>;
-  const double nzc = (double)C::NZ * N * N;
   RG_CUDA_TRY(ctx, prep(k_hii_x<N>, smem_x<N>()));
   prof_begin(ctx, "inv_x_c2c_window", st);
   k_hii_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smem_x<N>(), st>>>(spec, stride, ng, work, nr, wrows, wpitch,
@@ -501,7 +525,9 @@ size_t hii_bit_words() {
 template <int N>
 int launch_debug_inverse(rg_context* ctx, const cf* spec, cf* work, const float* wrow, float* out, cudaStream_t st) {
   const size_t stride = (size_t)Cfg<N>::NZ * N * N;
-  int rc = launch_inverse_xy<N>(ctx, spec, 1, work, stride, 1, wrow, 0, wrow ? -1 : 0, st);
+  int rc = xy_ctrl_reset(ctx, Cfg<N>::NZ, st);
+  if (rc) return rc;
+  rc = launch_inverse_xy<N>(ctx, spec, 1, work, stride, 1, wrow, 0, wrow ? -1 : 0, st);
   if (rc) return rc;
   const cf* tw;
   if ((rc = twiddles_for(ctx, N, &tw))) return rc;
@@ -581,6 +607,29 @@ int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int ns
   k_reduce_partials<<<1, 256, 0, st>>>(partials, nblocks, nsum, d_out);
   prof_end(ctx, 8.0 * nblocks * nsum, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
+  return RG_OK;
+}
+
+int xy_ctrl_reset(rg_context* ctx, size_t max_jobs, cudaStream_t st) {
+  const size_t need = max_jobs + 2;
+  if (!ctx->xy_ctrl || ctx->xy_ctrl_elems < need) {
+    if (ctx->xy_ctrl) cudaFree(ctx->xy_ctrl);
+    ctx->xy_ctrl = nullptr;
+    ctx->xy_ctrl_elems = 0;
+    cudaError_t e = cudaMalloc((void**)&ctx->xy_ctrl, sizeof(uint32_t) * need);
+    if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    ctx->xy_ctrl_elems = need;
+  }
+  RG_CUDA_TRY(ctx, cudaMemsetAsync(ctx->xy_ctrl, 0, sizeof(uint32_t), st));
+  return RG_OK;
+}
+
+int xy_ctrl_check(rg_context* ctx, cudaStream_t st) {
+  if (!ctx->xy_ctrl) return RG_OK;
+  uint32_t err = 0;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(&err, ctx->xy_ctrl, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (err) return set_error(ctx, RG_ETIMEDOUT, "fused x/y pass: a wait for the x pass of a plane ran out");
   return RG_OK;
 }
 
@@ -670,6 +719,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   hs.bits = ctx->bits;
   hs.partials = partials;
 
+  if ((rc = xy_ctrl_reset(ctx, (size_t)(N / 2 + 1) * kb, st))) return rc;
   int nblocks = 0;
   for (int r0 = 0; r0 < nr; r0 += kb) {
     const int cnt = std::min(kb, nr - r0);
@@ -702,6 +752,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * HII_NSUM, cudaMemcpyDeviceToHost, st));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   prof_resolve(ctx);
+  if ((rc = xy_ctrl_check(ctx, st))) return rc;
 
   const double n3 = std::pow((double)N, 3);
   const double* S = ctx->h_sums;
@@ -717,6 +768,10 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
   out->n_radii = nr;
   return RG_OK;
+}
+
+static int debug_inverse(rg_context* ctx, int n, const float* wrow, float* d_out, cudaStream_t st) {
+  RG_DISPATCH_N(n, launch_debug_inverse<NN>(ctx, ctx->spec, ctx->work, wrow, d_out, st));
 }
 
 int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype) {
@@ -737,7 +792,8 @@ int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, floa
     if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, 1, ftype, ctx->wtab, n2max, st))) return rc;
     wrow = ctx->wtab;
   }
-  RG_DISPATCH_N(N, launch_debug_inverse<NN>(ctx, ctx->spec, ctx->work, wrow, d_out, st));
+  if ((rc = debug_inverse(ctx, N, wrow, d_out, st))) return rc;
+  return xy_ctrl_check(ctx, st);
 }
 
 }  // namespace rg

@@ -106,6 +106,12 @@ int validate_common(rg_context* ctx, const rg_params* p);
 
 int twiddles_for(rg_context* ctx, int n, const cf** out);
 
+// Control words of the fused x/y passes: xy_ctrl_reset sizes them for up to max_jobs jobs per
+// launch and clears the error word (once per snapshot); xy_ctrl_check copies the error word to
+// the host after a stream sync and returns RG_ETIMEDOUT when a wait ran out.
+int xy_ctrl_reset(rg_context* ctx, size_t max_jobs, cudaStream_t st);
+int xy_ctrl_check(rg_context* ctx, cudaStream_t st);
+
 // Per-kernel event timing (active when ctx->prof_on).  prof_begin records a start event on
 // the stream; prof_end records the stop event and the launch's algorithmic bytes.
 void prof_begin(rg_context* ctx, const char* name, cudaStream_t st);
@@ -153,6 +159,10 @@ struct rg_context {
   size_t ts_sums_elems = 0;
   char* ts_const = nullptr;      // ComputeTs device constants and per-shell coefficients
   size_t ts_const_elems = 0;
+  // fused x/y pass control words: [0] error word, [1] item counter, [2 ..) per-job counts
+  uint32_t* xy_ctrl = nullptr;
+  size_t xy_ctrl_elems = 0;
+  int num_sms = 0;
   // profiling
   bool prof_on = false;
   struct ProfRec {

@@ -1,0 +1,218 @@
+// The inverse x and y passes of a batch of filtered grids as ONE persistent kernel whose
+// intermediate plane stays in L2.
+//
+// A job is one kz plane of one radius (or shell) of the batch, over all of the batch's grids:
+// the x pass of the job (window x spectrum, c2c along x) writes the plane into the work buffer,
+// the y pass (c2c along y) transforms it there in place.  Run as two kernels over the whole
+// batch, every plane crosses HBM three times (x store, y load, y store); here the y pass of a
+// job is issued shortly after its x pass, so the y loads hit the x stores in L2 and the plane
+// reaches HBM once.
+//
+// Work items are handed out by one atomic counter in a fixed sequence of segments of M items
+// (M = N / B column groups or line groups):
+//
+//   X(0) .. X(L-1), X(L), Y(0), X(L+1), Y(1), ..., X(J-1), Y(J-L-1), Y(J-L) .. Y(J-1)
+//
+// (J jobs, lag L).  Jobs run kz-major, radius-minor, so a spectrum plane is read from HBM by the
+// first radius and from L2 by the others.  A Y item waits (thread 0, acquire load, bounded) until
+// all M X items of its job have signalled (release after a block barrier).  Every X item of a
+// job precedes its Y items in the sequence and X items wait on nothing, so the smallest
+// unfinished item can always finish: the kernel needs no co-resident grid and no cooperative
+// launch.  A wait that runs out sets the error word and the item goes on (the host reports
+// RG_ETIMEDOUT); no wait is unbounded.
+#pragma once
+
+#include <algorithm>
+
+#include "rg_internal.h"
+#include "rg_pass.cuh"
+
+namespace rg {
+
+struct XYSched {
+  int nr;            // radii (or shells) per kz plane
+  int M;             // items per segment
+  int J;             // jobs = (N/2 + 1) * nr
+  int L;             // lag of the Y segments behind the X segments, 1 <= L <= J
+  int total;         // 2 J M
+  uint32_t* ctr;     // item counter (zero at launch)
+  uint32_t* done;    // [J] finished X items per job (zero at launch)
+  uint32_t* err;     // set to 1 when a wait runs out
+};
+
+__device__ __forceinline__ void xy_decode(const XYSched& s, int seg, bool& is_y, int& job) {
+  if (seg < s.L) {
+    is_y = false;
+    job = seg;
+    return;
+  }
+  const int u = seg - s.L;
+  const int mid = 2 * (s.J - s.L);
+  if (u < mid) {
+    is_y = (u & 1) != 0;
+    job = is_y ? (u >> 1) : s.L + (u >> 1);
+  } else {
+    is_y = true;
+    job = s.J - s.L + (u - mid);
+  }
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// thread 0 only: wait until job's X items have all signalled (at most ~2^22 polls)
+__device__ __forceinline__ void xy_wait(const XYSched& s, int job) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    if (ld_acquire_u32(s.done + job) >= (uint32_t)s.M) return;
+    __nanosleep(64);
+  }
+  atomicExch(s.err, 1u);
+}
+
+template <int N>
+struct XYF {
+  static constexpr int T = Cfg<N>::T;
+  static constexpr int V = Cfg<N>::V;
+  static constexpr int B = Cfg<N>::BX;   // columns per X item, lines per Y item
+  static constexpr int NTH = T * B;
+  static constexpr int M = N / B;
+  static constexpr int XBUF = cmax(line_buf<N, B>(), B * Cfg<N>::PITCH_P);
+  static constexpr size_t smem() { return sizeof(cf) * (size_t)(N + XBUF); }
+};
+
+__device__ __forceinline__ cf ldcg_cf(const cf* p) {
+  const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+  return cf{v.x, v.y};
+}
+
+// release the finished X item: the block barrier before it orders the block's stores
+__device__ __forceinline__ void xy_signal(uint32_t* p) {
+  __threadfence();
+  atomicAdd(p, 1u);
+}
+
+// Op (by value) describes the batch:
+//   int grids() const                         grids per job
+//   int nsrc(int r) const                     spectra combined into each grid of radius r
+//   const cf* src(int r, int g, int i) const  spectrum i of grid g (layout S[kz][x][y])
+//   float coef(int r, int i) const            its coefficient
+//   bool filtered(int r) const                radius r is windowed
+//   const float* wrow(int r) const            its window row W[n2]
+//   cf* out(int r, int g) const               output grid (plane kz at kz N^2)
+// The X input of grid g is W(k) * sum_i coef_i src_i(k), accumulated in the order of i with fmaf.
+template <int N, class Op>
+__global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
+    k_xy_fused(XYSched sch, Op op, const cf* __restrict__ g_tw) {
+  constexpr int T = XYF<N>::T, B = XYF<N>::B, V = XYF<N>::V;
+  extern __shared__ cf smem[];
+  cf* s_tw = smem;
+  cf* xbuf = smem + N;
+  __shared__ int s_item[2];
+  load_twiddles<N>(s_tw, g_tw);
+  if (threadIdx.x == 0) s_item[0] = (int)atomicAdd(sch.ctr, 1u);
+  __syncthreads();
+  int it = 0;
+  int item = s_item[0];
+  const int ng = op.grids();
+  while (item < sch.total) {
+    int nxt = 0;
+    if (threadIdx.x == 0) nxt = (int)atomicAdd(sch.ctr, 1u);   // the next item, fetched early
+    const int seg = item / sch.M, k = item - seg * sch.M;
+    bool is_y;
+    int job;
+    xy_decode(sch, seg, is_y, job);
+    const int kz = job / sch.nr, r = job - kz * sch.nr;
+    const size_t plane = (size_t)kz * N * N;
+    if (!is_y) {
+      const int b = threadIdx.x % B, t = threadIdx.x / B;
+      const int y = k * B + b;
+      const size_t col = plane + y;
+      float wv[V];
+#pragma unroll
+      for (int sl = 0; sl < V; ++sl) wv[sl] = 1.f;
+      if (op.filtered(r)) {
+        const float* wr = op.wrow(r);
+        const int ny = y > N / 2 ? y - N : y;
+#pragma unroll
+        for (int sl = 0; sl < V; ++sl) {
+          const int p = stage0_pos<N>(t, sl);
+          const int nx = p > N / 2 ? p - N : p;
+          wv[sl] = __ldg(wr + (nx * nx + ny * ny + kz * kz));
+        }
+      }
+      const int ns = op.nsrc(r);
+      for (int g = 0; g < ng; ++g) {
+        cf* dst = op.out(r, g);
+        line_fft<N, true>(
+            t, xbuf, s_tw,
+            [&](int p, int sl) {
+              float ax = 0.f, ay = 0.f;
+              for (int i = 0; i < ns; ++i) {
+                const float c = op.coef(r, i);
+                const float2 v = __ldg(reinterpret_cast<const float2*>(op.src(r, g, i) + col + (size_t)p * N));
+                ax = fmaf(c, v.x, ax);
+                ay = fmaf(c, v.y, ay);
+              }
+              return cf{ax * wv[sl], ay * wv[sl]};
+            },
+            [&](int p) { return line_addr<N, B>(p, b); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
+      }
+      __syncthreads();   // every store of the item is issued
+      if (threadIdx.x == 0) xy_signal(sch.done + job);
+    } else {
+      if (threadIdx.x == 0) xy_wait(sch, job);
+      __syncthreads();
+      const int t = threadIdx.x % T, b = threadIdx.x / T;
+      const size_t row = plane + (size_t)(k * B + b) * N;
+      for (int g = 0; g < ng; ++g) {
+        cf* line = op.out(r, g) + row;
+        line_fft<N, true>(
+            t, xbuf, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return pos_addr<N>(b, p); },
+            [&](int p, cf v) { line[p] = v; });
+      }
+    }
+    if (threadIdx.x == 0) s_item[(it + 1) & 1] = nxt;
+    __syncthreads();
+    ++it;
+    item = s_item[it & 1];
+  }
+}
+
+// Launch the fused pass of one batch of nr radii (or shells); the control words must have been
+// sized by xy_ctrl_reset for at least (N/2 + 1) nr jobs.
+template <int N, class Op>
+int launch_xy_fused(rg_context* ctx, const Op& op, int nr, const char* name, double alg_bytes, cudaStream_t st) {
+  using F = XYF<N>;
+  const cf* tw;
+  int rc = twiddles_for(ctx, N, &tw);
+  if (rc) return rc;
+  const int J = Cfg<N>::NZ * nr;
+  if (nr < 1 || (size_t)J + 2 > ctx->xy_ctrl_elems) return set_error(ctx, RG_EINVAL, "fused x/y pass: batch too large");
+  auto kern = k_xy_fused<N, Op>;
+  RG_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F::smem()));
+  int per_sm = 0;
+  RG_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, F::NTH, F::smem()));
+  const int grid = std::max(per_sm, 1) * ctx->num_sms;
+  XYSched s;
+  s.nr = nr;
+  s.M = F::M;
+  s.J = J;
+  // Y(j) is handed out (2L + 1) M items after X(j) starts; with `grid` blocks in flight that is
+  // about when X(j) completes for L = grid / (2M), one more for slack
+  s.L = std::min(J, (grid + 2 * F::M - 1) / (2 * F::M) + 1);
+  s.total = 2 * J * F::M;
+  s.err = ctx->xy_ctrl;
+  s.ctr = ctx->xy_ctrl + 1;
+  s.done = ctx->xy_ctrl + 2;
+  RG_CUDA_TRY(ctx, cudaMemsetAsync(s.ctr, 0, sizeof(uint32_t) * ((size_t)J + 1), st));
+  prof_begin(ctx, name, st);
+  kern<<<std::min(grid, s.total), F::NTH, F::smem(), st>>>(s, op, tw);
+  prof_end(ctx, alg_bytes, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  return RG_OK;
+}
+
+}  // namespace rg
