@@ -785,11 +785,6 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   if (!no_light) {
     if (!s->stored_fcoll && s->snapshot > 0)
       return set_error(ctx, RG_EINVAL, "ComputeTs needs stored_fcoll of the previous snapshot");
-    TsTables tb;
-    std::string msg;
-    if ((rc = ts_tables(p, ctx->tables, sh, zp, x_e_ave, collapse_fraction, s->ZZ, s->stored_fcoll, s->snapshot, &tb,
-                        &msg)))
-      return set_error(ctx, rc, msg);
     // sources used by any shell
     std::vector<int> slot_of(sh.nsrc, -1), used;
     for (int r = 0; r < nS; ++r)
@@ -840,6 +835,37 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     if ((rc = ensure_mem(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nS * (n2max + 1)))) return rc;
     if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, nS, p->TsHeatingFilterType, ctx->wtab, n2max, st))) return rc;
 
+    // x and y passes in batches of TS_KB shells into work[r][g]
+    for (int r0 = 0; r0 < nS; r0 += TS_KB) {
+      const int cnt = std::min(TS_KB, nS - r0);
+      TsBatch bt;
+      std::memset(&bt, 0, sizeof(bt));
+      bt.nr = cnt;
+      for (int j = 0; j < cnt; ++j) {
+        const int r = r0 + j;
+        int nk = 0;
+        for (int k = 0; k < sh.nsrc; ++k) {
+          const float c = sh.coef[(size_t)r * sh.nsrc + k];
+          if (c != 0.f) {
+            bt.ks[j][nk] = slot_of[k];
+            bt.cs[j][nk] = c;
+            nk++;
+          }
+        }
+        bt.nk[j] = nk;
+        bt.filtered[j] = r > 0;  // no filter on the first shell (ComputeTs.c:529)
+        bt.wrow[j] = r;
+      }
+      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, st)))
+        return rc;
+    }
+    // the frequency tables on the host while the device runs the transforms above
+    TsTables tb;
+    std::string msg;
+    if ((rc = ts_tables(p, ctx->tables, sh, zp, x_e_ave, collapse_fraction, s->ZZ, s->stored_fcoll, s->snapshot, &tb,
+                        &msg)))
+      return set_error(ctx, rc, msg);
+
     // per-shell coefficients.  evolveInt sums over shells R (XRayHeatingFunctions.c:1379-1432):
     //   heat/ion/lya: dt_dzpp dzpp XRAY_R (1+zpp)^-alpha fi_k(x_e)     (times const_zp later)
     //   star        : SFR_R (1+zp)^2 (1+zpp) sum_lyn dt_dzpp dzpp      (times the conversion)
@@ -887,30 +913,6 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       hco[r].cstar = (float)(cs[r] * scale[3]);
     }
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(d_co, hco.data(), sizeof(TsShellCoef) * (nS + 1), cudaMemcpyHostToDevice, st));
-    // x and y passes in batches of TS_KB shells into work[r][g]
-    for (int r0 = 0; r0 < nS; r0 += TS_KB) {
-      const int cnt = std::min(TS_KB, nS - r0);
-      TsBatch bt;
-      std::memset(&bt, 0, sizeof(bt));
-      bt.nr = cnt;
-      for (int j = 0; j < cnt; ++j) {
-        const int r = r0 + j;
-        int nk = 0;
-        for (int k = 0; k < sh.nsrc; ++k) {
-          const float c = sh.coef[(size_t)r * sh.nsrc + k];
-          if (c != 0.f) {
-            bt.ks[j][nk] = slot_of[k];
-            bt.cs[j][nk] = c;
-            nk++;
-          }
-        }
-        bt.nk[j] = nk;
-        bt.filtered[j] = r > 0;  // no filter on the first shell (ComputeTs.c:529)
-        bt.wrow[j] = r;
-      }
-      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, st)))
-        return rc;
-    }
     zv.nS = nS;
     if ((rc = ensure_mem(ctx, &ctx->ts_sums, &ctx->ts_sums_elems, n3))) return rc;
     if ((rc = ts_zsum(ctx, N, ctx->work, nc, d_co, zv, g->x_e_box_prev, ctx->ts_sums, st))) return rc;
