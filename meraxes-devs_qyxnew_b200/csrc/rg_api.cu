@@ -286,6 +286,10 @@ int rg_create(int device, int grid_dim, rg_context** out) {
     return RG_ECUDA;
   }
   ctx->stream = ctx->own_stream;
+  if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    rg_destroy(ctx);
+    return RG_ECUDA;
+  }
   if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
       ctx->num_sms < 1) {
     rg_destroy(ctx);
@@ -320,6 +324,11 @@ int rg_destroy(rg_context* ctx) {
   for (void* p : ctx->owned) cudaFree(p);
   prof_resolve(ctx);
   for (cudaEvent_t e : ctx->prof_pool) cudaEventDestroy(e);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  for (cudaEvent_t e : ctx->stage_events) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return RG_OK;
@@ -425,9 +434,10 @@ int rg_init_reion_grids(rg_context* ctx, const rg_params* p, const rg_grids* g) 
   return RG_OK;
 }
 
-int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
-                        rg_hii_scalars* out) {
-  if (!ctx || !p || !s || !g || !out || !s->ZZ) return RG_EINVAL;
+}  // extern "C"
+
+static int find_hii(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+                    rg_hii_scalars* out, const Staging* stg) {
   int rc = validate_common(ctx, p);
   if (rc) return rc;
   if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return set_error(ctx, RG_EINVAL, "snapshot out of range");
@@ -447,12 +457,54 @@ int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* 
     return set_error(ctx, RG_EINVAL, "BH feedback needs effective_bhm and effective_bhar");
   if ((rc = ensure_tables(ctx, p))) return rc;
   cudaSetDevice(ctx->device);
-  return hii_snapshot(ctx, p, s, g, out);
+  return hii_snapshot(ctx, p, s, g, out, stg);
 }
 
-static int copy_grid(rg_context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+// event i of the context's staging pool (created on first use)
+static cudaEvent_t stage_event(rg_context* ctx, size_t i) {
+  while (ctx->stage_events.size() <= i) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    ctx->stage_events.push_back(e);
+  }
+  return ctx->stage_events[i];
+}
+
+int rg::stage_wait(rg_context* ctx, cudaEvent_t ev, cudaStream_t st) {
+  if (ev) RG_CUDA_TRY(ctx, cudaStreamWaitEvent(st, ev, 0));
+  return RG_OK;
+}
+
+int rg::stage_record(rg_context* ctx, size_t i, cudaStream_t st, cudaEvent_t* out) {
+  cudaEvent_t e = stage_event(ctx, i);
+  if (!e) return set_error(ctx, RG_ECUDA, "cudaEventCreate failed");
+  RG_CUDA_TRY(ctx, cudaEventRecord(e, st));
+  *out = e;
+  return RG_OK;
+}
+
+// the copy stream starts after the work already queued on the context's stream (which may
+// still read the device grids the copies overwrite)
+static int copy_stream_after_prior(rg_context* ctx) {
+  cudaEvent_t e;
+  int rc = stage_record(ctx, 0, ctx->stream, &e);
+  if (rc) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, e, 0));
+  return RG_OK;
+}
+
+extern "C" {
+
+int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+                        rg_hii_scalars* out) {
+  if (!ctx || !p || !s || !g || !out || !s->ZZ) return RG_EINVAL;
+  return find_hii(ctx, p, s, g, out, nullptr);
+}
+
+static int copy_grid(rg_context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,
+                     cudaStream_t st = nullptr) {
   if (!dst || !src) return RG_OK;
-  RG_CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, bytes, kind, ctx->stream));
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, bytes, kind, st ? st : ctx->stream));
   return RG_OK;
 }
 
@@ -476,7 +528,7 @@ static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
 
 int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* h,
                              rg_hii_scalars* out) {
-  if (!ctx || !p || !s || !h || !out) return RG_EINVAL;
+  if (!ctx || !p || !s || !h || !out || !s->ZZ) return RG_EINVAL;
   int rc = validate_common(ctx, p);
   if (rc) return rc;
   cudaSetDevice(ctx->device);
@@ -485,28 +537,39 @@ int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snaps
   const size_t n = (size_t)ctx->N;
   const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float), br = n * n * n * sizeof(float);
   const auto H2D = cudaMemcpyHostToDevice;
-  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D))) return rc;
-  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D))) return rc;
-  if ((rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D))) return rc;
-  if ((rc = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D))) return rc;
-  if ((rc = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D))) return rc;
-  if ((rc = copy_grid(ctx, d.temp_kinetic_all_gas, h->temp_kinetic_all_gas, br, H2D))) return rc;
-  if (p->Flag_IncludeSpinTemp) {
-    if ((rc = copy_grid(ctx, d.x_e_box, h->x_e_box, bp, H2D))) return rc;
-    if ((rc = copy_grid(ctx, d.Tk_box, h->Tk_box, br, H2D))) return rc;
+  cudaStream_t cs = ctx->copy_stream;
+  const bool plain = ctx->mode == RG_MODE_PLAIN;
+  // uploads in the order the snapshot reads them: the transformed grids, the ionisation state
+  // (first z pass), the closing-pass grids; each group's event gates its first reader
+  Staging stg;
+  if ((rc = copy_stream_after_prior(ctx))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D, cs))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D, cs))) return rc;
+  if (p->Flag_IncludeSpinTemp && (rc = copy_grid(ctx, (void*)d.x_e_box, h->x_e_box, bp, H2D, cs))) return rc;
+  if (p->Flag_BHFeedback && (rc = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D, cs))) return rc;
+  if (plain && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
+  if ((rc = stage_record(ctx, 1, cs, &stg.inputs))) return rc;
+  if ((rc = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D, cs))) return rc;
+  if ((rc = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D, cs))) return rc;
+  if ((rc = stage_record(ctx, 2, cs, &stg.state))) return rc;
+  if ((rc = copy_grid(ctx, d.temp_kinetic_all_gas, h->temp_kinetic_all_gas, br, H2D, cs))) return rc;
+  if (p->Flag_IncludeSpinTemp && (rc = copy_grid(ctx, (void*)d.Tk_box, h->Tk_box, br, H2D, cs))) return rc;
+  if (!plain && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
+  if (p->Flag_BHFeedback && (rc = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D, cs))) return rc;
+  if ((rc = stage_record(ctx, 3, cs, &stg.closing))) return rc;
+  stg.host_r_bubble = h->r_bubble;
+  rc = find_hii(ctx, p, s, &d, out, &stg);
+  if (rc) {
+    cudaStreamSynchronize(cs);   // no copy of the caller's arrays outlives the call
+    return rc;
   }
-  if (p->Flag_BHFeedback) {
-    if ((rc = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D))) return rc;
-    if ((rc = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D))) return rc;
-  }
-  if ((rc = rg_find_HII_bubbles(ctx, p, s, &d, out))) return rc;
   const auto D2H = cudaMemcpyDeviceToHost;
   if ((rc = copy_grid(ctx, h->xH, d.xH, br, D2H))) return rc;
-  if ((rc = copy_grid(ctx, h->r_bubble, d.r_bubble, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(cs));
   return RG_OK;
 }
 
@@ -576,7 +639,7 @@ int rg_profile_read(rg_context* ctx, rg_kernel_stat* out, int max, int* n) {
 }
 
 static int compute_ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
-                      const rg_grids* src_host, rg_ts_scalars* out) {
+                      const rg_grids* src_host, rg_ts_scalars* out, const Staging* stg = nullptr) {
   int rc = validate_common(ctx, p);
   if (rc) return rc;
   if (!s->ZZ) return set_error(ctx, RG_EINVAL, "ZZ is required");
@@ -600,7 +663,7 @@ static int compute_ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s,
     return set_error(ctx, RG_EINVAL, "ComputeTs needs the sfr and xray_luminosity grids");
   if ((rc = ensure_tables(ctx, p))) return rc;
   cudaSetDevice(ctx->device);
-  rc = ts_snapshot(ctx, p, s, g, out, src_host);
+  rc = ts_snapshot(ctx, p, s, g, out, src_host, stg);
   if (rc == RG_OK && s->stored_fcoll) s->stored_fcoll[s->snapshot] = out->collapse_fraction;
   return rc;
 }
@@ -622,18 +685,28 @@ int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   const size_t n = (size_t)ctx->N;
   const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float), br = n * n * n * sizeof(float);
   const auto H2D = cudaMemcpyHostToDevice;
-  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D))) return rc;
-  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D))) return rc;
-  if ((rc = copy_grid(ctx, d.x_e_box_prev, h->x_e_box_prev, bp, H2D))) return rc;
-  if ((rc = copy_grid(ctx, d.Tk_box, h->Tk_box, br, H2D))) return rc;
-  // the source grids are staged from h inside the step (only the history slots in use)
-  if ((rc = compute_ts(ctx, p, s, &d, h, out))) return rc;
+  cudaStream_t cs = ctx->copy_stream;
+  // deltax, stars and x_e_box_prev feed the first reduction; Tk_box only the evolution step.
+  // The source grids are staged from h inside the step (only the history slots in use).
+  Staging stg;
+  if ((rc = copy_stream_after_prior(ctx))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D, cs))) return rc;
+  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D, cs))) return rc;
+  if ((rc = copy_grid(ctx, d.x_e_box_prev, h->x_e_box_prev, bp, H2D, cs))) return rc;
+  if ((rc = stage_record(ctx, 1, cs, &stg.inputs))) return rc;
+  if ((rc = copy_grid(ctx, d.Tk_box, h->Tk_box, br, H2D, cs))) return rc;
+  if ((rc = stage_record(ctx, 3, cs, &stg.closing))) return rc;
+  if ((rc = compute_ts(ctx, p, s, &d, h, out, &stg))) {
+    cudaStreamSynchronize(cs);   // no copy of the caller's arrays outlives the call
+    return rc;
+  }
   const auto D2H = cudaMemcpyDeviceToHost;
   if ((rc = copy_grid(ctx, h->x_e_box_prev, d.x_e_box_prev, bp, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->x_e_box, d.x_e_box, bp, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->Tk_box, d.Tk_box, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->TS_box, d.TS_box, br, D2H))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(cs));
   return RG_OK;
 }
 

@@ -648,7 +648,10 @@ static int ensure_buf(rg_context* ctx, T** ptr, size_t* have, size_t need) {
 // ---------------------------------------------------------------------------
 // the snapshot
 
-int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out) {
+int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out,
+                 const Staging* stg) {
+  const Staging none;
+  if (!stg) stg = &none;
   int rc;
   cudaStream_t st = ctx->stream;
   const int N = ctx->N;
@@ -691,6 +694,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc * ng * kb))) return rc;
   const size_t nw = bit_words(N);
   if ((rc = ensure_buf(ctx, &ctx->bits, &ctx->bits_elems, 2 * nw))) return rc;
+  if ((rc = stage_wait(ctx, stg->inputs, st))) return rc;
   if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
 
   // window table for all radii
@@ -704,6 +708,14 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
 
   // r_bubble is only written on the recombination branch: zero it once
   RG_CUDA_TRY(ctx, cudaMemsetAsync(g->r_bubble, 0, sizeof(float) * (size_t)N * N * N, st));
+  if (stg->host_r_bubble) {
+    // final already: the host copy overlaps the radius loop
+    cudaEvent_t e;
+    if ((rc = stage_record(ctx, 4, st, &e))) return rc;
+    RG_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, e, 0));
+    RG_CUDA_TRY(ctx, cudaMemcpyAsync(stg->host_r_bubble, g->r_bubble, sizeof(float) * (size_t)N * N * N,
+                                     cudaMemcpyDeviceToHost, ctx->copy_stream));
+  }
   double* partials = ensure_partials(ctx, (size_t)N * N * HII_NSUM);
   if (!partials) return set_error(ctx, RG_ENOMEM, "partials");
 
@@ -746,6 +758,8 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     if ((rc = inverse_xy(ctx, N, ctx->spec, ng, ctx->work, nc, cnt, ctx->wtab + (size_t)r0 * (n2max + 1), n2max + 1,
                          unf, st)))
       return rc;
+    if (r0 == 0 && (rc = stage_wait(ctx, stg->state, st))) return rc;
+    if (fin && (rc = stage_wait(ctx, stg->closing, st))) return rc;
     if ((rc = hii_z(ctx, N, ctx->work, nc, ntest, bt, c, hs, fin, st, &nblocks))) return rc;
   }
   if ((rc = reduce_partials(ctx, partials, nblocks, HII_NSUM, ctx->d_sums, st))) return rc;

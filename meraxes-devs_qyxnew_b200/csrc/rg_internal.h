@@ -90,13 +90,30 @@ int fft_forward(rg_context* ctx, int n, const float* const* d_real, int ng, cf* 
 // W[r][n2] for the radii in d_radii (filter() closed forms, double precision)
 int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int ftype, float* d_wtab, int n2max,
                  cudaStream_t st);
+// Uploads still in flight on the context's copy stream when a snapshot is enqueued (the host
+// entry points): each stage of the snapshot waits for the event of the grids it reads or
+// overwrites, so the copies overlap the work that needs none of them.  Null events are ready.
+struct Staging {
+  cudaEvent_t inputs = nullptr;    // grids of the forward transforms (Ts: also of the first reduction)
+  cudaEvent_t state = nullptr;     // find_HII: z_at_ionization, J_21_at_ionization (first z pass)
+  cudaEvent_t closing = nullptr;   // find_HII: temperature, Tk_box, weighted_sfr, effective_bhar
+                                   // (closing pass); Ts: Tk_box (the evolution step)
+  float* host_r_bubble = nullptr;  // find_HII: copy r_bubble here on the copy stream once zeroed
+};
+int stage_wait(rg_context* ctx, cudaEvent_t ev, cudaStream_t st);
+// record event i of the context's staging pool on st (events 0-3 are used by the host entry
+// points, 4 and up by the source groups of ComputeTs)
+int stage_record(rg_context* ctx, size_t i, cudaStream_t st, cudaEvent_t* out);
+
 // The excursion-set step on device grids (rg_hii.cu).
-int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out);
+int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out,
+                 const Staging* stg = nullptr);
 // The spin-temperature step on device grids (rg_ts.cu).  With src_host, the sfr /
 // xray_luminosity grids and their histories are read from those HOST arrays instead of g, and
-// only the history slots the shells use are copied to the device.
+// only the history slots the shells use are copied to the device (on the copy stream, one
+// event per group of forward transforms).
 int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_ts_scalars* out,
-                const rg_grids* src_host = nullptr);
+                const rg_grids* src_host = nullptr, const Staging* stg = nullptr);
 // Forward + (windowed) inverse of one padded grid, for tests.
 int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype);
 int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out, cudaStream_t st);
@@ -163,6 +180,9 @@ struct rg_context {
   uint32_t* xy_ctrl = nullptr;
   size_t xy_ctrl_elems = 0;
   int num_sms = 0;
+  // host entry points: uploads and early downloads run on copy_stream, ordered by these events
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> stage_events;
   // profiling
   bool prof_on = false;
   struct ProfRec {

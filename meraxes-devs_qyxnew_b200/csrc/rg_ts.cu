@@ -664,8 +664,10 @@ static double pow2_scale(double maxabs) {
 }
 
 int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_ts_scalars* out,
-                const rg_grids* src_host) {
+                const rg_grids* src_host, const Staging* stg) {
   int rc;
+  const Staging none;
+  if (!stg) stg = &none;
   cudaStream_t st = ctx->stream;
   const int N = ctx->N;
   const size_t n3 = (size_t)N * N * N;
@@ -746,6 +748,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
 
   // collapse fraction and <x_e> (both branches compute the collapse fraction)
   prof_begin(ctx, "ts_reduce0", st);
+  if ((rc = stage_wait(ctx, stg->inputs, st))) return rc;
   k_ts_reduce0<<<nblk, 256, 0, st>>>(g->stars, g->deltax, g->x_e_box_prev, N, Mh2, ftpr3, partials);
   prof_end(ctx, 12.0 * n3, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
@@ -761,6 +764,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     const float xe0 = (float)xion_RECFAST(ctx->tables, (float)zp);
     const float TK0 = (float)T_RECFAST(ctx->tables, (float)zp);
     prof_begin(ctx, "ts_homog", st);
+    if ((rc = stage_wait(ctx, stg->closing, st))) return rc;   // Tk_box is overwritten
     k_ts_homog<<<nblk, 256, 0, st>>>(d_hc, xe0, TK0, cT_approx((float)zp), N, g->deltax, g->x_e_box_prev,
                                       g->x_e_box, g->Tk_box, g->TS_box, partials, d_nonconv);
     prof_end(ctx, 28.0 * n3, st);
@@ -808,26 +812,10 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       if (k == 0) return which ? sg->xray_luminosity : sg->sfr;
       return (which ? sg->xray_luminosity_histories : sg->sfr_histories) + (size_t)(k - 1) * npad;
     };
-    if (src_host) {
-      if ((rc = ensure_mem(ctx, &ctx->ts_stage, &ctx->ts_stage_elems, npad * 2 * used.size()))) return rc;
-      for (size_t j = 0; j < used.size(); ++j)
-        for (int which = 0; which < 2; ++which)
-          RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ts_stage + (j * 2 + which) * npad, src_grid(used[j], which),
-                                           sizeof(float) * npad, cudaMemcpyHostToDevice, st));
-    }
+    if (src_host && (rc = ensure_mem(ctx, &ctx->ts_stage, &ctx->ts_stage_elems, npad * 2 * used.size()))) return rc;
     auto dev_grid = [&](size_t j, int which) -> const float* {
       return src_host ? ctx->ts_stage + (j * 2 + which) * npad : src_grid(used[j], which);
     };
-    // forward transforms of the used sources: spec[(slot * 2 + g)]
-    for (size_t i = 0; i < used.size(); i += 4) {
-      const float* srcs[8];
-      int ng = 0;
-      for (size_t j = i; j < used.size() && j < i + 4; ++j) {
-        srcs[ng++] = dev_grid(j, 0);
-        srcs[ng++] = dev_grid(j, 1);
-      }
-      if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec + nc * 2 * i, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
-    }
     // window rows for the shells (filter() takes BoxSize in Mpc/h and R in Mpc, ComputeTs.c:532)
     const int n2max = 3 * (N / 2) * (N / 2);
     if ((rc = ensure_mem(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nS))) return rc;
@@ -835,9 +823,38 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     if ((rc = ensure_mem(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nS * (n2max + 1)))) return rc;
     if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, nS, p->TsHeatingFilterType, ctx->wtab, n2max, st))) return rc;
 
-    // x and y passes in batches of TS_KB shells into work[r][g]
+    // Batches of TS_KB shells: the forward transforms of the sources a batch uses first (`used`
+    // is in order of first use), then its x and y passes into work[r][g].  From host arrays,
+    // each group of sources is copied on the copy stream and its transform waits for the copy,
+    // so the copies of later sources overlap the passes of earlier batches.
+    size_t next_slot = 0;   // used[0, next_slot) are transformed into spec[slot * 2 + g]
     for (int r0 = 0; r0 < nS; r0 += TS_KB) {
       const int cnt = std::min(TS_KB, nS - r0);
+      size_t need = next_slot;
+      for (int r = r0; r < r0 + cnt; ++r)
+        for (int k = 0; k < sh.nsrc; ++k)
+          if (sh.coef[(size_t)r * sh.nsrc + k] != 0.f) need = std::max(need, (size_t)slot_of[k] + 1);
+      while (next_slot < need) {
+        const size_t end = std::min(need, next_slot + 4);
+        if (src_host) {
+          for (size_t j = next_slot; j < end; ++j)
+            for (int which = 0; which < 2; ++which)
+              RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ts_stage + (j * 2 + which) * npad, src_grid(used[j], which),
+                                               sizeof(float) * npad, cudaMemcpyHostToDevice, ctx->copy_stream));
+          cudaEvent_t e;
+          if ((rc = stage_record(ctx, 4 + next_slot, ctx->copy_stream, &e))) return rc;
+          if ((rc = stage_wait(ctx, e, st))) return rc;
+        }
+        const float* srcs[8];
+        int ng = 0;
+        for (size_t j = next_slot; j < end; ++j) {
+          srcs[ng++] = dev_grid(j, 0);
+          srcs[ng++] = dev_grid(j, 1);
+        }
+        if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec + nc * 2 * next_slot, nc, 1.0 / std::pow((double)N, 3), st)))
+          return rc;
+        next_slot = end;
+      }
       TsBatch bt;
       std::memset(&bt, 0, sizeof(bt));
       bt.nr = cnt;
@@ -932,6 +949,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   e.no_light = no_light;
   const double4 inv = make_double4(zv.inv_scale[0], zv.inv_scale[1], zv.inv_scale[2], zv.inv_scale[3]);
   prof_begin(ctx, "ts_evolve", st);
+  if ((rc = stage_wait(ctx, stg->closing, st))) return rc;
   k_ts_evolve<<<nblk, 256, 0, st>>>(d_hc, e, inv, N, no_light ? nullptr : ctx->ts_sums, g->deltax, g->x_e_box_prev,
                                      g->x_e_box, g->Tk_box, g->TS_box, partials, d_nonconv);
   prof_end(ctx, (double)n3 * (16 + 4 + 4 + 4 + 4 + 4 + 4 + 4), st);

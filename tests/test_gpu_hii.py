@@ -156,25 +156,49 @@ def test_plain_mode_matches_fused_large(n, box):
     assert 0.0 < oa.volume_weighted_global_xH < 1.0
 
 
-def test_host_entry_point_matches_device():
+@pytest.mark.parametrize("mode,spin", [(rg.RG_MODE_FUSED, False), (rg.RG_MODE_PLAIN, False), (rg.RG_MODE_FUSED, True)])
+def test_host_entry_point_matches_device(mode, spin):
+    """The host-buffer entry point (uploads on the copy stream, gated per stage) gives the device
+    entry point's grids and scalars bit for bit."""
     n, box, z = 32, 32.0, 8.0
     src = wl.make_sources(n, box, seed=11)
-    dg, out, p = run_gpu_hii(n, box, z, src, 4000.0)
-    h = {k: np.zeros(n ** 3, np.float32) for k in ("xH", "r_bubble", "J_21_at_ionization", "temp_kinetic_all_gas")}
-    h["z_at_ionization"] = np.full(n ** 3, -1.0, np.float32)
-    g = rg.rg_grids()
-    keep = {"deltax": np.ascontiguousarray(src.deltax), "stars": np.ascontiguousarray(src.stars),
-            "weighted_sfr": np.ascontiguousarray(src.sfr)}
-    keep.update(h)
-    for k, v in keep.items():
-        setattr(g, k, v.ctypes.data)
+    rng = np.random.default_rng(5)
+    npad = n * n * 2 * (n // 2 + 1)
+    xe = (rng.random(npad) * 0.05).astype(np.float32)
+    tk = (20.0 + 10.0 * rng.random(n ** 3)).astype(np.float32)
+    kw = {"Flag_IncludeSpinTemp": 1} if spin else {}
+    p = rg.make_params(n, box, Flag_EvolvingReionRBubbleMax=0, ReionRBubbleMax=50.0, ReionEfficiency=4000.0, **kw)
     zz, snap = wl.snapshot_redshifts(z)
     s = rg.snapshot(zz, snap)
+    dg = DeviceGrids(n, spin=spin)
+    dg.put("deltax", src.deltax)
+    dg.put("stars", src.stars)
+    dg.put("weighted_sfr", src.sfr)
+    if spin:
+        dg.put("x_e_box", xe)
+        dg.put("Tk_box", tk)
     ctx = rg.Context(n)
+    ctx.call("rg_set_mode", mode)
+    out = rg.rg_hii_scalars()
+    ctx.call("rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out))
+    ctx.close()
+    h = {k: np.zeros(n ** 3, np.float32) for k in ("xH", "r_bubble", "J_21_at_ionization", "temp_kinetic_all_gas")}
+    h["r_bubble"][:] = 7.0   # overwritten with zeros
+    h["z_at_ionization"] = np.full(n ** 3, -1.0, np.float32)
+    keep = {"deltax": np.ascontiguousarray(src.deltax), "stars": np.ascontiguousarray(src.stars),
+            "weighted_sfr": np.ascontiguousarray(src.sfr)}
+    if spin:
+        keep.update(x_e_box=xe, Tk_box=tk)
+    keep.update(h)
+    g = rg.rg_grids()
+    for k, v in keep.items():
+        setattr(g, k, v.ctypes.data)
+    ctx = rg.Context(n)
+    ctx.call("rg_set_mode", mode)
     o2 = rg.rg_hii_scalars()
     ctx.call("rg_find_HII_bubbles_host", C.byref(p), C.byref(s), C.byref(g), C.byref(o2))
     ctx.close()
-    for k in ("xH", "z_at_ionization", "J_21_at_ionization", "temp_kinetic_all_gas"):
+    for k in ("xH", "z_at_ionization", "J_21_at_ionization", "temp_kinetic_all_gas", "r_bubble"):
         assert np.array_equal(h[k].reshape(n, n, n), dg.get(k)), k
     assert o2.as_dict() == out.as_dict()
 
