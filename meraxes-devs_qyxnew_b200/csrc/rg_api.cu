@@ -313,6 +313,7 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->work) cudaFree(ctx->work);
   if (ctx->bits) cudaFree(ctx->bits);
   if (ctx->wtab) cudaFree(ctx->wtab);
+  if (ctx->wcut) cudaFree(ctx->wcut);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);

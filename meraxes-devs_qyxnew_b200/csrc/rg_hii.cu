@@ -29,8 +29,17 @@ namespace rg {
 // window table W[r][n2], n2 = nx^2 + ny^2 + nz^2, evaluated in double from the closed
 // forms of filter() (src/core/reionization.c:3404-3428)
 
+// sharp-k: k R 0.413566994 > 1 zeroes the mode
+__device__ __forceinline__ bool sharpk_zero(double delta_k, int n2, double R) {
+  const double kR = delta_k * sqrt((double)n2) * R;
+  return kR * 0.413566994 > 1.0;
+}
+
+// For the sharp-k filter (ftype 1) the row is a step in n2 (kR grows with n2); wcut[r], when
+// given, receives the last n2 of the step (written by that entry alone), so
+// W[r][n2] == (n2 <= wcut[r]).
 __global__ void k_window_table(float* wtab, int n2max, const double* __restrict__ radii, int nr, double delta_k,
-                               int ftype) {
+                               int ftype, int* wcut) {
   const int r = blockIdx.y;
   if (r >= nr) return;
   const double R = radii[r];
@@ -40,12 +49,13 @@ __global__ void k_window_table(float* wtab, int n2max, const double* __restrict_
     if (ftype == 0) {
       if (kR > 1e-4) w = 3.0 * (sin(kR) / (kR * kR * kR) - cos(kR) / (kR * kR));
     } else if (ftype == 1) {
-      if (kR * 0.413566994 > 1.0) w = 0.0;
+      if (sharpk_zero(delta_k, n2, R)) w = 0.0;
     } else {
       const double g = kR * 0.643;
       w = exp(-g * g / 2.0);
     }
     wtab[(size_t)r * (n2max + 1) + n2] = (float)w;
+    if (ftype == 1 && wcut && w == 1.0 && (n2 == n2max || sharpk_zero(delta_k, n2 + 1, R))) wcut[r] = n2;
   }
 }
 
@@ -439,12 +449,14 @@ struct HiiXOp {
   const float* wrows;
   int wpitch;
   int unfiltered;
+  const int* wcut;   // sharp-k step ends per radius, or null (window rows are read)
   __device__ int grids() const { return ng; }
   __device__ int nsrc(int) const { return 1; }
   __device__ const cf* src(int, int g, int) const { return spec + g * stride; }
   __device__ float coef(int, int) const { return 1.f; }
   __device__ bool filtered(int r) const { return r != unfiltered; }
   __device__ const float* wrow(int r) const { return wrows + (size_t)r * wpitch; }
+  __device__ int cutoff(int r) const { return wcut ? __ldg(wcut + r) : -2; }
   __device__ cf* out(int r, int g) const { return work + ((size_t)r * ng + g) * stride; }
 };
 
@@ -452,11 +464,11 @@ struct HiiXOp {
 // passes as separate kernels
 template <int N>
 int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, cf* work, size_t stride, int nr, const float* wrows,
-                      int wpitch, int unfiltered, cudaStream_t st) {
+                      int wpitch, int unfiltered, cudaStream_t st, const int* wcut = nullptr) {
   using C = Cfg<N>;
   const double nzc = (double)C::NZ * N * N;
   if (ctx->mode == RG_MODE_FUSED) {
-    const HiiXOp op{spec, stride, ng, work, wrows, wpitch, unfiltered};
+    const HiiXOp op{spec, stride, ng, work, wrows, wpitch, unfiltered, wcut};
     return launch_xy_fused<N>(ctx, op, nr, "inv_xy_c2c_window", ng * 8.0 * nzc * (1 + nr), st);
   }
   const cf* tw;
@@ -580,8 +592,8 @@ int fft_forward(rg_context* ctx, int n, const float* const* d_real, int ng, cf* 
 }
 
 static int inverse_xy(rg_context* ctx, int n, const cf* spec, int ng, cf* work, size_t stride, int nr,
-                      const float* wrows, int wpitch, int unfiltered, cudaStream_t st) {
-  RG_DISPATCH_N(n, launch_inverse_xy<NN>(ctx, spec, ng, work, stride, nr, wrows, wpitch, unfiltered, st));
+                      const float* wrows, int wpitch, int unfiltered, cudaStream_t st, const int* wcut) {
+  RG_DISPATCH_N(n, launch_inverse_xy<NN>(ctx, spec, ng, work, stride, nr, wrows, wpitch, unfiltered, st, wcut));
 }
 
 static int hii_z(rg_context* ctx, int n, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
@@ -592,11 +604,12 @@ static int hii_z(rg_context* ctx, int n, const cf* work, size_t stride, int ng, 
 static size_t bit_words(int n) { RG_DISPATCH_N_VAL(n, hii_bit_words<NN>(), (size_t)0); }
 
 int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int ftype, float* d_wtab, int n2max,
-                 cudaStream_t st) {
+                 cudaStream_t st, int* d_wcut) {
   const double delta_k = 2.0 * M_PI / box;
   const int bx = (n2max + 1 + 255) / 256;
+  if (ftype != 1) d_wcut = nullptr;
   prof_begin(ctx, "window_table", st);
-  k_window_table<<<dim3(bx < 1024 ? bx : 1024, nr), 256, 0, st>>>(d_wtab, n2max, d_radii, nr, delta_k, ftype);
+  k_window_table<<<dim3(bx < 1024 ? bx : 1024, nr), 256, 0, st>>>(d_wtab, n2max, d_radii, nr, delta_k, ftype, d_wcut);
   prof_end(ctx, 4.0 * (n2max + 1) * nr, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
@@ -704,7 +717,10 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   if ((rc = ensure_buf(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
   if ((rc = ensure_buf(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
-  if ((rc = window_table(ctx, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st))) return rc;
+  if ((rc = ensure_buf(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nr))) return rc;
+  if ((rc = window_table(ctx, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st, ctx->wcut)))
+    return rc;
+  const int* wcut = p->ReionFilterType == 1 ? ctx->wcut : nullptr;
 
   // r_bubble is only written on the recombination branch: zero it once
   RG_CUDA_TRY(ctx, cudaMemsetAsync(g->r_bubble, 0, sizeof(float) * (size_t)N * N * N, st));
@@ -756,7 +772,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     // the snapshot's last radius is unfiltered (find_HII_bubbles.c:313)
     const int unf = fin ? cnt - 1 : -1;
     if ((rc = inverse_xy(ctx, N, ctx->spec, ng, ctx->work, nc, cnt, ctx->wtab + (size_t)r0 * (n2max + 1), n2max + 1,
-                         unf, st)))
+                         unf, st, wcut ? wcut + r0 : nullptr)))
       return rc;
     if (r0 == 0 && (rc = stage_wait(ctx, stg->state, st))) return rc;
     if (fin && (rc = stage_wait(ctx, stg->closing, st))) return rc;

@@ -87,9 +87,10 @@ constexpr int KB_MAX = 16;    // radii per batch
 // Forward r2c of ng padded real grids into spectra spec_base + g * stride, scaled.
 int fft_forward(rg_context* ctx, int n, const float* const* d_real, int ng, cf* spec_base, size_t stride,
                 double scale, cudaStream_t st);
-// W[r][n2] for the radii in d_radii (filter() closed forms, double precision)
+// W[r][n2] for the radii in d_radii (filter() closed forms, double precision); for the sharp-k
+// filter also d_wcut[r] (when given), the last n2 of the step, so W[r][n2] == (n2 <= d_wcut[r])
 int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int ftype, float* d_wtab, int n2max,
-                 cudaStream_t st);
+                 cudaStream_t st, int* d_wcut = nullptr);
 // Uploads still in flight on the context's copy stream when a snapshot is enqueued (the host
 // entry points): each stage of the snapshot waits for the event of the grids it reads or
 // overwrites, so the copies overlap the work that needs none of them.  Null events are ready.
@@ -157,6 +158,8 @@ struct rg_context {
   size_t bits_elems = 0;
   float* wtab = nullptr;         // window table [nR][n2max+1]
   size_t wtab_elems = 0;
+  int* wcut = nullptr;           // sharp-k window: last n2 of each row's step
+  size_t wcut_elems = 0;
   double* partials = nullptr;
   size_t partials_elems = 0;
   double* d_sums = nullptr;      // reduced sums

@@ -201,7 +201,7 @@ struct TsBatch {
 template <int N>
 __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, (x_pass_minb<N>()))
     k_ts_x(const cf* __restrict__ spec, size_t stride, cf* __restrict__ work, TsBatch bt,
-           const float* __restrict__ wtab, int wpitch, const cf* __restrict__ g_tw) {
+           const float* __restrict__ wtab, int wpitch, const int* __restrict__ wcut, const cf* __restrict__ g_tw) {
   constexpr int T = Cfg<N>::T, B = Cfg<N>::BX, V = Cfg<N>::V;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
@@ -226,9 +226,16 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, (x_pass_minb<N>()))
 #pragma unroll
       for (int sl = 0; sl < V; ++sl) wv[sl] = 1.f;
     } else {
-      const float* wr = wtab + (size_t)bt.wrow[r] * wpitch;
+      if (wcut) {
+        // sharp-k: the row is the step W = (n2 <= cut), no gathers
+        const int cut = __ldg(wcut + bt.wrow[r]);
 #pragma unroll
-      for (int sl = 0; sl < V; ++sl) wv[sl] = __ldg(wr + n2[sl]);
+        for (int sl = 0; sl < V; ++sl) wv[sl] = n2[sl] <= cut ? 1.f : 0.f;
+      } else {
+        const float* wr = wtab + (size_t)bt.wrow[r] * wpitch;
+#pragma unroll
+        for (int sl = 0; sl < V; ++sl) wv[sl] = __ldg(wr + n2[sl]);
+      }
     }
     const int nk = bt.nk[r];
     for (int g = 0; g < 2; ++g) {
@@ -594,7 +601,7 @@ static int ensure_mem(rg_context* ctx, T** ptr, size_t* have, size_t need) {
 // x and y passes of a batch of shells: work_base + (j * 2 + g) * stride, j < bt.nr
 template <int N>
 static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
-                        const float* wtab, int wpitch, cudaStream_t st) {
+                        const float* wtab, int wpitch, const int* wcut, cudaStream_t st) {
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
@@ -603,7 +610,7 @@ static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t s
   const size_t smx = sizeof(cf) * (N + (size_t)line_buf<N, C::BX>());
   RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_x<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
   prof_begin(ctx, "ts_x_c2c_combine_window", st);
-  k_ts_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smx, st>>>(spec, stride, work_base, bt, wtab, wpitch, tw);
+  k_ts_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smx, st>>>(spec, stride, work_base, bt, wtab, wpitch, wcut, tw);
   double src_reads = 0;
   for (int r = 0; r < bt.nr; ++r) src_reads += bt.nk[r];
   prof_end(ctx, 2 * 8.0 * nzc * (src_reads + bt.nr), st);
@@ -649,8 +656,8 @@ static int launch_ts_zsum(rg_context* ctx, const cf* work, size_t stride, const 
   }
 
 static int ts_xy(rg_context* ctx, int n, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
-                 const float* wtab, int wpitch, cudaStream_t st) {
-  RG_TS_DISPATCH(n, launch_ts_xy<NN>(ctx, spec, work_base, stride, bt, wtab, wpitch, st));
+                 const float* wtab, int wpitch, const int* wcut, cudaStream_t st) {
+  RG_TS_DISPATCH(n, launch_ts_xy<NN>(ctx, spec, work_base, stride, bt, wtab, wpitch, wcut, st));
 }
 
 static int ts_zsum(rg_context* ctx, int n, const cf* work, size_t stride, const TsShellCoef* d_co, const TsZev& zv,
@@ -821,7 +828,11 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     if ((rc = ensure_mem(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nS))) return rc;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, sh.R.data(), sizeof(double) * nS, cudaMemcpyHostToDevice, st));
     if ((rc = ensure_mem(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nS * (n2max + 1)))) return rc;
-    if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, nS, p->TsHeatingFilterType, ctx->wtab, n2max, st))) return rc;
+    if ((rc = ensure_mem(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nS))) return rc;
+    if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, nS, p->TsHeatingFilterType, ctx->wtab, n2max, st,
+                           ctx->wcut)))
+      return rc;
+    const int* wcut = p->TsHeatingFilterType == 1 ? ctx->wcut : nullptr;
 
     // Batches of TS_KB shells: the forward transforms of the sources a batch uses first (`used`
     // is in order of first use), then its x and y passes into work[r][g].  From host arrays,
@@ -873,7 +884,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
         bt.filtered[j] = r > 0;  // no filter on the first shell (ComputeTs.c:529)
         bt.wrow[j] = r;
       }
-      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, st)))
+      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, wcut, st)))
         return rc;
     }
     // the frequency tables on the host while the device runs the transforms above

@@ -101,6 +101,8 @@ __device__ __forceinline__ void xy_signal(uint32_t* p) {
 //   float coef(int r, int i) const            its coefficient
 //   bool filtered(int r) const                radius r is windowed
 //   const float* wrow(int r) const            its window row W[n2]
+//   int cutoff(int r) const                   >= -1: the row is the step W = (n2 <= cutoff), read
+//                                             without gathers (sharp-k); < -1: read the row
 //   cf* out(int r, int g) const               output grid (plane kz at kz N^2)
 // The X input of grid g is W(k) * sum_i coef_i src_i(k), accumulated in the order of i with fmaf.
 template <int N, class Op>
@@ -135,12 +137,14 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
       for (int sl = 0; sl < V; ++sl) wv[sl] = 1.f;
       if (op.filtered(r)) {
         const float* wr = op.wrow(r);
+        const int cut = op.cutoff(r);
         const int ny = y > N / 2 ? y - N : y;
 #pragma unroll
         for (int sl = 0; sl < V; ++sl) {
           const int p = stage0_pos<N>(t, sl);
           const int nx = p > N / 2 ? p - N : p;
-          wv[sl] = __ldg(wr + (nx * nx + ny * ny + kz * kz));
+          const int n2 = nx * nx + ny * ny + kz * kz;
+          wv[sl] = cut >= -1 ? (n2 <= cut ? 1.f : 0.f) : __ldg(wr + n2);
         }
       }
       const int ns = op.nsrc(r);

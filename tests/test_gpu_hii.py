@@ -124,15 +124,15 @@ def test_find_hii_bubbles_config_efficiency():
     assert out.volume_weighted_global_xH > 0.99
 
 
-def compare_modes(n, box, z, seed, eff=4000.0):
+def compare_modes(n, box, z, seed, eff=4000.0, ftype=0):
     """The fused mode (radius batches, windowed inverse passes, two-for-one c2r) against the plain
     mode (one FFT chain per grid per radius, every reference grid).  Both are FP32 evaluations of
     the same sums; where the compiler contracts them differently the rounding differs, so:
     ionised flags differ in <= 0.01% of cells, J_21 and the temperatures agree to 1e-5 relative L2,
     the box averages to 1e-5."""
     src = wl.make_sources(n, box, seed=seed)
-    a, oa, _ = run_gpu_hii(n, box, z, src, eff, mode=rg.RG_MODE_FUSED)
-    b, ob, _ = run_gpu_hii(n, box, z, src, eff, mode=rg.RG_MODE_PLAIN)
+    a, oa, _ = run_gpu_hii(n, box, z, src, eff, ftype, mode=rg.RG_MODE_FUSED)
+    b, ob, _ = run_gpu_hii(n, box, z, src, eff, ftype, mode=rg.RG_MODE_PLAIN)
     ia, ib = a.get("xH") < ro.REL_TOL, b.get("xH") < ro.REL_TOL
     assert (ia != ib).mean() <= 1e-4
     same = ia == ib
@@ -148,6 +148,12 @@ def compare_modes(n, box, z, seed, eff=4000.0):
 
 def test_plain_mode_matches_fused():
     compare_modes(64, 64.0, 8.0, 5)
+
+
+def test_plain_mode_matches_fused_sharp_k():
+    # the fused pass applies the sharp-k window as the step n2 <= cutoff, the plain pass reads
+    # the window table: both are the same window
+    compare_modes(128, 128.0, 8.0, 8, ftype=1)
 
 
 @pytest.mark.parametrize("n,box", [(256, 250.0), (512, 500.0)])
