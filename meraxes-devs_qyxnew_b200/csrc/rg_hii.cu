@@ -195,10 +195,29 @@ struct HiiState {
   double* partials;          // [nblocks][HII_NSUM]
 };
 
+// Shared-memory plan of the z pass: ZB tile buffers of TB complex each; the buffer of the unit
+// being transformed is also its FFT exchange buffer (the tile is consumed by the first stage).
+// Two buffers let the next grid's tile arrive while this one is transformed.  At 512^3 the
+// batches before the last use one buffer instead, which brings a block to 72 KB and 77 registers
+// and the SM to three blocks (measured: 46.0 -> 44.0 ms over 7 batches; the closing batch, with
+// more registers, keeps two buffers).
+template <int N, bool FINAL>
+struct HiiZ {
+  static constexpr int NTH = Cfg<N>::T * Cfg<N>::QZ;
+  static constexpr bool WIDE = N == 512 && !FINAL;
+  static constexpr int ZB = WIDE ? 1 : 2;
+  static constexpr int TB = round_up(cmax((int)ztile_elems<N>(), line_buf<N, Cfg<N>::QZ>()), 2);
+  static constexpr int MINB = WIDE ? 3 : RG_MINB(NTH);
+  static constexpr size_t smem(int ng) {
+    return sizeof(cf) * (size_t)N + sizeof(float) * (size_t)round_up(ng * 2 * Cfg<N>::QZ * Cfg<N>::RT_PITCH, 4) +
+           sizeof(cf) * (size_t)ZB * TB;
+  }
+};
+
 // z pass of a batch.  FINAL: the batch ends with the snapshot's last (unfiltered) radius.
 // Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then effective_bhm (BH).
 template <int N, int NG, bool FINAL>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<N>::QZ))
+__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
     k_hii_z(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
             HiiState s) {
   constexpr int T = Cfg<N>::T, Q = Cfg<N>::QZ, NTH = T * Q, ROWS = 2 * Q, RP = Cfg<N>::RT_PITCH;
@@ -208,10 +227,11 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<
   static_assert(ROWS * N % NTH == 0, "whole rows per block");
   extern __shared__ __align__(16) unsigned char smem_raw[];  // 16-byte aligned for cp.async
   cf* smem = reinterpret_cast<cf*>(smem_raw);
+  constexpr int ZB = HiiZ<N, FINAL>::ZB, TB = HiiZ<N, FINAL>::TB;
   cf* s_tw = smem;
-  cf* xbuf = smem + N;
-  float* rt = reinterpret_cast<float*>(xbuf + line_buf<N, Q>());
-  // two shared tiles: grid u + 1 is copied while grid u is transformed
+  float* rt = reinterpret_cast<float*>(smem + N);
+  // ZB shared tiles (with two, grid u + 1 is copied while grid u is transformed); the tile of
+  // unit u is the exchange buffer of its transform
   cf* tiles = reinterpret_cast<cf*>(rt + round_up(NG * ROWS * RP, 4));
   const int x = blockIdx.y, y0 = blockIdx.x * ROWS;
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
@@ -254,20 +274,28 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, RG_MINB(Cfg<N>::T* Cfg<
 #pragma unroll 1
     for (int g = 0; g < NG; ++g) {
       const int u = r * NG + g;
-      if (u + 1 < nunits) ztile_issue<N, Q>(tiles + ((u + 1) & 1) * ztile_elems<N>(), work + (size_t)(u + 1) * stride, x, y0, NTH);
-      cp_async_commit();
-      cp_async_wait<1>();
+      cf* tile = tiles + (ZB == 2 ? (u & 1) : 0) * TB;
+      if constexpr (ZB == 2) {
+        if (u + 1 < nunits) ztile_issue<N, Q>(tiles + ((u + 1) & 1) * TB, work + (size_t)(u + 1) * stride, x, y0, NTH);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
       __syncthreads();  // unit u's tile is complete for every thread
-      const cf* tile = tiles + (u & 1) * ztile_elems<N>();
       float* r0 = rt + (size_t)(g * ROWS + 2 * q) * RP;
       line_fft<N, true>(
-          tq, xbuf, s_tw, [&](int p, int) { return ztile_c2r_input<N, Q>(tile, q, p); },
+          tq, tile, s_tw, [&](int p, int) { return ztile_c2r_input<N, Q>(tile, q, p); },
           [&](int p) { return line_addr<N, Q>(p, q); },
           [&](int p, cf v) {
             r0[p] = v.x;
             r0[RP + p] = v.y;
           });
-      __syncthreads();  // the tile is consumed before unit u + 2 refills it; rt row is written
+      __syncthreads();  // the tile is consumed before it is refilled; rt row is written
+      if constexpr (ZB == 1) {
+        if (u + 1 < nunits) ztile_issue<N, Q>(tiles, work + (size_t)(u + 1) * stride, x, y0, NTH);
+        cp_async_commit();
+      }
     }
     const bool last = FINAL && r == bt.nr - 1;
     const double pref = bt.fcoll_pref[r];
@@ -495,8 +523,7 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
-  const size_t sm = sizeof(cf) * (N + (size_t)line_buf<N, C::QZ>()) +
-                    sizeof(float) * (size_t)round_up(NG * 2 * C::QZ * C::RT_PITCH, 4) + sizeof(cf) * 2 * ztile_elems<N>();
+  const size_t sm = HiiZ<N, FINAL>::smem(NG);
   RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL>, sm));
   const dim3 grid(N / (2 * C::QZ), N);
   // algorithmic bytes: the Hermitian halves of NG grids per radius, z_at_ionization on the
