@@ -542,6 +542,25 @@ def run_ours(args, cfg):
                                         "GBps": k["alg_bytes_total"] / max(k["ms_total"], 1e-9) / 1e6}
                             for k in stats}}
 
+    # the 21-cm power spectrum of the step's delta_T (Compute_PS, run after the step by the
+    # reference when Flag_ComputePS is set): not part of the metric, timed on its own
+    extras = {}
+    if wk.spin:
+        dptr = wk.b["delta_T"].data_ptr()
+        ctx.power_spectrum(wk.p, dptr)
+        torch.cuda.synchronize(dev)
+        pst = []
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ps_k, ps_d, _ = ctx.power_spectrum(wk.p, dptr)
+            e1.record(stream)
+            e1.synchronize()
+            pst.append(e0.elapsed_time(e1))
+        extras["power_spectrum"] = {"ms": statistics.mean(pst), "bins": int(len(ps_k)),
+                                    "what": "Compute_PS of delta_T on the device, host outputs"}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         ms_cpu, desc, wall, _ = cpu_sample(cfg, src, ti, zz, snap)
@@ -553,7 +572,7 @@ def run_ours(args, cfg):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, BASELINE shapes)",
                 "config": dict(workload_desc(cfg, nr), mode=args.mode, parallelism=f"replicas x{ws}"),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clk, "results": results}
+                "clocks": clk, "results": results, "extras": extras}
         print(json.dumps(line), flush=True)
     ctx.close()
     if ws > 1:

@@ -178,6 +178,27 @@ int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
 int rg_delta_T_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* host,
                     double* volume_ave_Tb);
 
+/* ---- callers next to the step ---- */
+
+/* Number of k bins of the 21-cm power spectrum (PS_Length): Initialise_PowerSpectrum
+   (src/core/ComputePowerSpectrum.c:18-42).  Needs ReionGridDim, BoxSize and Hubble_h. */
+int rg_power_spectrum_length(const rg_params* p, int* n_bins);
+/* Compute_PS (src/core/ComputePowerSpectrum.c:44-255) of the device grid delta_T (REAL layout,
+   N^3 floats): fills PS_k, PS_data and PS_error (HOST arrays of at least max_bins floats) and
+   *n_bins; an empty bin gives NaN there as in the reference.  Mini-halo (delta_TII) channels
+   are not built. */
+int rg_power_spectrum(rg_context* ctx, const rg_params* p, const float* d_delta_T, int max_bins, float* PS_k,
+                      float* PS_data, float* PS_error, int* n_bins);
+/* The same from a HOST delta_T (the reion_grids_t array). */
+int rg_power_spectrum_host(rg_context* ctx, const rg_params* p, const float* h_delta_T, int max_bins,
+                           float* PS_k, float* PS_data, float* PS_error, int* n_bins);
+/* smooth_grid (src/core/read_grids.c:127-165): a padded grid of the context's dimension (the
+   finer grid read from file) is transformed, divided by N^3, filtered with the real-space
+   top-hat of radius (float)(box_size / reion_grid_dim / 2) and transformed back (device
+   pointers; in place allowed). */
+int rg_smooth_grid(rg_context* ctx, double box_size, int reion_grid_dim, const float* d_in_padded,
+                   float* d_out_padded);
+
 /* ---- per-kernel timing: CUDA events on the launching stream around every launch ---- */
 typedef struct rg_kernel_stat {
   char name[48];

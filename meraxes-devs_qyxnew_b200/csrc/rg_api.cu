@@ -314,6 +314,8 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->bits) cudaFree(ctx->bits);
   if (ctx->wtab) cudaFree(ctx->wtab);
   if (ctx->wcut) cudaFree(ctx->wcut);
+  if (ctx->ps_pad) cudaFree(ctx->ps_pad);
+  if (ctx->ps_stage) cudaFree(ctx->ps_stage);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);

@@ -160,6 +160,10 @@ struct rg_context {
   size_t wtab_elems = 0;
   int* wcut = nullptr;           // sharp-k window: last n2 of each row's step
   size_t wcut_elems = 0;
+  float* ps_pad = nullptr;       // power spectrum: padded real input of the transform
+  size_t ps_pad_elems = 0;
+  float* ps_stage = nullptr;     // power spectrum from host delta_T: its device copy
+  size_t ps_stage_elems = 0;
   double* partials = nullptr;
   size_t partials_elems = 0;
   double* d_sums = nullptr;      // reduced sums

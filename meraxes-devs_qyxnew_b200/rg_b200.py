@@ -113,6 +113,12 @@ _SIGS = {
     "rg_compute_Ts_host": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_snapshot), _P(rg_grids), _P(rg_ts_scalars)]),
     "rg_delta_T_host": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_snapshot), _P(rg_grids), _P(C.c_double)]),
     "rg_debug_filter_roundtrip": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_void_p, C.c_double, C.c_int]),
+    "rg_power_spectrum_length": (C.c_int, [_P(rg_params), _P(C.c_int)]),
+    "rg_power_spectrum": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_int, _P(C.c_float), _P(C.c_float),
+                                    _P(C.c_float), _P(C.c_int)]),
+    "rg_power_spectrum_host": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_int, _P(C.c_float),
+                                         _P(C.c_float), _P(C.c_float), _P(C.c_int)]),
+    "rg_smooth_grid": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
     "rg_radius_schedule": (C.c_int, [_P(rg_params), C.c_double, _P(C.c_double), C.c_int, _P(C.c_int)]),
     "rg_debug_ts_tables": (C.c_int, [_P(rg_params), _P(rg_snapshot), C.c_int, C.c_double, C.c_double, C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -160,6 +166,13 @@ def make_params(n: int, box: float, **kw) -> rg_params:
             raise AttributeError(k)
         setattr(p, k, v)
     return p
+
+
+def power_spectrum_length(p: rg_params) -> int:
+    """PS_Length of Initialise_PowerSpectrum (host computation)."""
+    n = C.c_int()
+    check(None, load().rg_power_spectrum_length(C.byref(p), C.byref(n)))
+    return n.value
 
 
 def radius_schedule(p: rg_params, redshift: float, max_r: int = 4096):
@@ -227,6 +240,18 @@ class Context:
 
     def call(self, name, *args):
         check(self.h, getattr(self.lib, name)(self.h, *args))
+
+    def power_spectrum(self, p: rg_params, delta_T_ptr: int, host: bool = False, max_bins: int = 64):
+        """Compute_PS of delta_T (a device pointer, or a host pointer with host=True): returns
+        (PS_k, PS_data, PS_error) as float32 arrays."""
+        import numpy as np
+        k, d, e = (C.c_float * max_bins)(), (C.c_float * max_bins)(), (C.c_float * max_bins)()
+        n = C.c_int()
+        self.call("rg_power_spectrum_host" if host else "rg_power_spectrum", C.byref(p), C.c_void_p(delta_T_ptr),
+                  max_bins, k, d, e, C.byref(n))
+        m = n.value
+        return (np.frombuffer(k, np.float32)[:m].copy(), np.frombuffer(d, np.float32)[:m].copy(),
+                np.frombuffer(e, np.float32)[:m].copy())
 
     def profile(self, on: bool):
         self.call("rg_profile_enable", int(on))
