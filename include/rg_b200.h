@@ -68,6 +68,9 @@ typedef struct rg_params {
   int Flag_IncludePecVelsFor21cm;
   /* directory holding recfast_LCDM.dat, kappa_*_table.dat, stellar_spectra.dat, x_int_tables/ */
   const char* TablesForXHeatingDir;
+  /* merger-tree code of the velocity grid (meraxes.h:253-258): 0 VELOCIraptor, 1 gbpTrees,
+     2 VELOCIraptor (augmented); sets the units of rg_grids.vel */
+  int TreesID;
 } rg_params;
 
 /* Fill *p with the values of input/params/defaults.par and the Genesis cosmology/units. */
@@ -102,6 +105,10 @@ typedef struct rg_grids {
   int n_hist;
   /* brightness temperature output, real [N]^3 */
   float* delta_T;
+  /* line-of-sight (z) velocity, padded, in the tree code's units; read by the brightness
+     temperature when Flag_IncludePecVelsFor21cm > 0.  The reference converts this grid in
+     place (BrightnessTemperature.c:173-196); the library leaves it unchanged. */
+  const float* vel;
 } rg_grids;
 
 /* The snapshot being processed: run_globals.ZZ[] and the snapshot index into it. */
@@ -163,7 +170,10 @@ int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* 
 /* _ComputeTs (src/core/ComputeTs.c:85-1554). */
 int rg_compute_Ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
                   rg_ts_scalars* out);
-/* ComputeBrightnessTemperatureBox (src/core/BrightnessTemperature.c:24-549); writes *volume_ave_Tb. */
+/* ComputeBrightnessTemperatureBox (src/core/BrightnessTemperature.c:24-549); writes *volume_ave_Tb.
+   With Flag_IncludeSpinTemp and Flag_IncludePecVelsFor21cm 1-3 it also applies the velocity
+   gradient (:198-305, reionization.c:3435-3450) and, for 3, the line-of-sight redshift-space
+   re-binning (:307-509); g->vel is then required. */
 int rg_delta_T(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
                double* volume_ave_Tb);
 

@@ -316,6 +316,8 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->wcut) cudaFree(ctx->wcut);
   if (ctx->ps_pad) cudaFree(ctx->ps_pad);
   if (ctx->ps_stage) cudaFree(ctx->ps_stage);
+  if (ctx->vel_work) cudaFree(ctx->vel_work);
+  if (ctx->vel_stage) cudaFree(ctx->vel_stage);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
@@ -398,6 +400,7 @@ int rg_alloc_grids(rg_context* ctx, const rg_params* p, int n_hist, rg_grids* ou
   RG_ALLOC(J_21_at_ionization, nreal);
   RG_ALLOC(temp_kinetic_all_gas, nreal);
   RG_ALLOC(delta_T, nreal);
+  if (p->Flag_IncludeSpinTemp && p->Flag_IncludePecVelsFor21cm > 0) RG_ALLOC(vel, npad);
   if (p->Flag_IncludeSpinTemp) {
     RG_ALLOC(x_e_box_prev, npad);
     RG_ALLOC(x_e_box, npad);

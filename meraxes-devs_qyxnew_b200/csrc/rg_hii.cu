@@ -831,6 +831,13 @@ static int debug_inverse(rg_context* ctx, int n, const float* wrow, float* d_out
   RG_DISPATCH_N(n, launch_debug_inverse<NN>(ctx, ctx->spec, ctx->work, wrow, d_out, st));
 }
 
+int spectrum_to_padded(rg_context* ctx, float* d_out, cudaStream_t st) {
+  const size_t nc = (size_t)(ctx->N / 2 + 1) * ctx->N * ctx->N;
+  int rc;
+  if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc))) return rc;
+  return debug_inverse(ctx, ctx->N, nullptr, d_out, st);
+}
+
 int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype) {
   int rc;
   cudaStream_t st = ctx->stream;

@@ -115,6 +115,9 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
 // event per group of forward transforms).
 int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_ts_scalars* out,
                 const rg_grids* src_host = nullptr, const Staging* stg = nullptr);
+// Unnormalised c2r of the spectrum in ctx->spec into a padded real grid (the context's inverse
+// passes, no window); the caller checks the fused pass's error word (xy_ctrl_check) after a sync.
+int spectrum_to_padded(rg_context* ctx, float* d_out, cudaStream_t st);
 // Forward + (windowed) inverse of one padded grid, for tests.
 int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, float* d_out, double R, int ftype);
 int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int nsum, double* d_out, cudaStream_t st);
@@ -164,6 +167,10 @@ struct rg_context {
   size_t ps_pad_elems = 0;
   float* ps_stage = nullptr;     // power spectrum from host delta_T: its device copy
   size_t ps_stage_elems = 0;
+  float* vel_work = nullptr;     // delta_T velocity modes: [converted velocity][its z gradient], padded
+  size_t vel_work_elems = 0;
+  float* vel_stage = nullptr;    // rg_delta_T_host: device copy of the caller's velocity grid
+  size_t vel_stage_elems = 0;
   double* partials = nullptr;
   size_t partials_elems = 0;
   double* d_sums = nullptr;      // reduced sums

@@ -40,6 +40,7 @@ class rg_params(C.Structure):
         ("SpecIndexXrayGal", C.c_double),
         ("Flag_IncludePecVelsFor21cm", C.c_int),
         ("TablesForXHeatingDir", C.c_char_p),
+        ("TreesID", C.c_int),
     ]
 
 
@@ -57,6 +58,7 @@ class rg_grids(C.Structure):
         ("sfr_histories", C.c_void_p), ("xray_luminosity_histories", C.c_void_p),
         ("n_hist", C.c_int),
         ("delta_T", C.c_void_p),
+        ("vel", C.c_void_p),
     ]
 
 
