@@ -560,6 +560,29 @@ def run_ours(args, cfg):
             pst.append(e0.elapsed_time(e1))
         extras["power_spectrum"] = {"ms": statistics.mean(pst), "bins": int(len(ps_k)),
                                     "what": "Compute_PS of delta_T on the device, host outputs"}
+        # delta_T with peculiar velocities and line-of-sight re-binning (flag 3) on a random
+        # velocity grid; not part of the metric
+        pv = rg.rg_params.from_buffer_copy(wk.p)
+        pv.Flag_IncludePecVelsFor21cm = 3
+        vel = torch.randn(wk.b["deltax"].numel(), device=dev) * 20.0
+        gv = rg.rg_grids.from_buffer_copy(wk.g)
+        gv.vel = vel.data_ptr()
+        tbv = C.c_double()
+        call = lambda: ctx.call("rg_delta_T", C.byref(pv), C.byref(wk.s), C.byref(gv), C.byref(tbv))
+        call()
+        torch.cuda.synchronize(dev)
+        vt = []
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            e1.synchronize()
+            vt.append(e0.elapsed_time(e1))
+        extras["delta_T_velocity_rsd"] = {"ms": statistics.mean(vt),
+                                          "what": "rg_delta_T with Flag_IncludePecVelsFor21cm 3 (random velocities)"}
+        del vel
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
