@@ -26,9 +26,10 @@ def _recfast():
     install_recfast()
 
 
-@pytest.mark.parametrize("n,box", [(8, 8.0), (16, 20.0), (24, 24.0), (32, 32.0), (48, 48.0), (64, 64.0),
-                                   (96, 96.0), (128, 100.0), (256, 250.0)])
-@pytest.mark.parametrize("ftype", [-1, 0, 1, 2])
+@pytest.mark.parametrize("n,box,ftype", [(n, b, f) for n, b in ((8, 8.0), (16, 20.0), (24, 24.0), (32, 32.0),
+                                                                 (48, 48.0), (64, 64.0), (96, 96.0), (128, 100.0),
+                                                                 (192, 190.0), (256, 250.0))
+                                          for f in (-1, 0, 1, 2)] + [(384, 380.0, 0), (512, 500.0, 0)])
 def test_filter_roundtrip_matches_fp64(n, box, ftype):
     import torch
     rng = np.random.default_rng(n * 7 + ftype)
@@ -156,7 +157,7 @@ def test_plain_mode_matches_fused_sharp_k():
     compare_modes(128, 128.0, 8.0, 8, ftype=1)
 
 
-@pytest.mark.parametrize("n,box", [(256, 250.0), (512, 500.0)])
+@pytest.mark.parametrize("n,box", [(192, 190.0), (256, 250.0), (512, 500.0)])
 def test_plain_mode_matches_fused_large(n, box):
     oa = compare_modes(n, box, 8.0, 6)
     assert 0.0 < oa.volume_weighted_global_xH < 1.0
