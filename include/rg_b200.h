@@ -188,6 +188,16 @@ int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
 int rg_delta_T_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* host,
                     double* volume_ave_Tb);
 
+/* The snapshot's reionization block (src/core/dracarys.c:383-391: call_ComputeTs when
+   Flag_IncludeSpinTemp, call_find_HII_bubbles, ComputeBrightnessTemperatureBox when
+   host->delta_T is non-null) in one call on HOST arrays, with the host grids of the three
+   _host entry points.  Each input is copied in once, in the order the steps read it, and
+   overlaps the work before its first reader; the grids passed from one step to the next stay on
+   the device; outputs are copied back as soon as they are final.  Outputs and scalars are those
+   of the three calls made one after another. */
+int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* host,
+                       rg_ts_scalars* ts, rg_hii_scalars* hii, double* volume_ave_Tb);
+
 /* ---- callers next to the step ---- */
 
 /* Number of k bins of the 21-cm power spectrum (PS_Length): Initialise_PowerSpectrum

@@ -286,7 +286,8 @@ int rg_create(int device, int grid_dim, rg_context** out) {
     return RG_ECUDA;
   }
   ctx->stream = ctx->own_stream;
-  if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->copy_stream_out, cudaStreamNonBlocking) != cudaSuccess) {
     rg_destroy(ctx);
     return RG_ECUDA;
   }
@@ -332,6 +333,10 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);
+  }
+  if (ctx->copy_stream_out) {
+    cudaStreamSynchronize(ctx->copy_stream_out);
+    cudaStreamDestroy(ctx->copy_stream_out);
   }
   for (cudaEvent_t e : ctx->stage_events) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -713,6 +718,101 @@ int rg_compute_Ts_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   if ((rc = copy_grid(ctx, h->TS_box, d.TS_box, br, D2H))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(cs));
+  return RG_OK;
+}
+
+// The snapshot's reionization block (dracarys.c:383-391): ComputeTs (with the spin temperature),
+// find_HII_bubbles and, when host->delta_T is given, ComputeBrightnessTemperatureBox, on the
+// HOST arrays.  Each input crosses PCIe once and in the order the steps read it (ComputeTs'
+// inputs, its history sources, then find_HII's state and closing-pass grids behind them on the
+// same copy stream); the grids the step hands from ComputeTs to find_HII_bubbles and to delta_T
+// (x_e_box, Tk_box, TS_box, deltax, xH) stay on the device; ComputeTs' outputs go back on a
+// second copy stream while find_HII_bubbles runs.
+int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* h,
+                       rg_ts_scalars* ts_out, rg_hii_scalars* hii_out, double* volume_ave_Tb) {
+  if (!ctx || !p || !s || !h || !hii_out || !s->ZZ) return RG_EINVAL;
+  const bool spin = p->Flag_IncludeSpinTemp != 0;
+  if (spin && !ts_out) return RG_EINVAL;
+  if (h->delta_T && !volume_ave_Tb) return RG_EINVAL;
+  int rc = validate_common(ctx, p);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  if ((rc = ensure_dev_grids(ctx, p, 0))) return rc;
+  const rg_grids& d = ctx->dev_grids;
+  const size_t n = (size_t)ctx->N;
+  const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float), br = n * n * n * sizeof(float);
+  const auto H2D = cudaMemcpyHostToDevice;
+  const auto D2H = cudaMemcpyDeviceToHost;
+  cudaStream_t cs = ctx->copy_stream, co = ctx->copy_stream_out, st = ctx->stream;
+  const bool plain = ctx->mode == RG_MODE_PLAIN;
+  auto fail = [&](int code) {
+    cudaStreamSynchronize(cs);   // no copy of the caller's arrays outlives the call
+    cudaStreamSynchronize(co);
+    return code;
+  };
+  // the velocity grid of delta_T's velocity modes goes to its own device buffer
+  const bool vel = h->delta_T && spin && p->Flag_IncludePecVelsFor21cm > 0;
+  if (vel && !h->vel) return set_error(ctx, RG_EINVAL, "missing grid pointer");
+  if (vel && (!ctx->vel_stage || ctx->vel_stage_elems < bp / sizeof(float))) {
+    if (ctx->vel_stage) cudaFree(ctx->vel_stage);
+    ctx->vel_stage = nullptr;
+    ctx->vel_stage_elems = 0;
+    if (cudaMalloc((void**)&ctx->vel_stage, bp) != cudaSuccess)
+      return set_error(ctx, RG_ENOMEM, "cudaMalloc of the velocity grid");
+    ctx->vel_stage_elems = bp / sizeof(float);
+  }
+  if ((rc = copy_stream_after_prior(ctx))) return rc;
+  RG_CUDA_TRY(ctx, cudaStreamWaitEvent(co, ctx->stage_events[0], 0));
+  Staging hs;   // find_HII's copies
+  // find_HII's own grids: the state for its first z pass, the closing-pass grids
+  auto hii_uploads = [&]() -> int {
+    int r;
+    if (plain && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
+    if (p->Flag_BHFeedback && (r = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D, cs))) return r;
+    if ((r = stage_record(ctx, 5, cs, &hs.inputs))) return r;
+    if ((r = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D, cs))) return r;
+    if ((r = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D, cs))) return r;
+    if ((r = stage_record(ctx, 6, cs, &hs.state))) return r;
+    if ((r = copy_grid(ctx, d.temp_kinetic_all_gas, h->temp_kinetic_all_gas, br, H2D, cs))) return r;
+    if (!plain && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
+    if (p->Flag_BHFeedback && (r = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D, cs))) return r;
+    if (vel && (r = copy_grid(ctx, ctx->vel_stage, h->vel, bp, H2D, cs))) return r;   // delta_T, after find_HII
+    return stage_record(ctx, 7, cs, &hs.closing);
+  };
+  if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D, cs))) return fail(rc);
+  if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D, cs))) return fail(rc);
+  if (spin) {
+    Staging ts;
+    if ((rc = copy_grid(ctx, d.x_e_box_prev, h->x_e_box_prev, bp, H2D, cs))) return fail(rc);
+    if ((rc = stage_record(ctx, 1, cs, &ts.inputs))) return fail(rc);
+    if ((rc = copy_grid(ctx, d.Tk_box, h->Tk_box, br, H2D, cs))) return fail(rc);
+    if ((rc = stage_record(ctx, 3, cs, &ts.closing))) return fail(rc);
+    ts.after_sources = hii_uploads;
+    if ((rc = compute_ts(ctx, p, s, &d, h, ts_out, &ts))) return fail(rc);
+    // ComputeTs' outputs go back while find_HII_bubbles runs (they are final, st is idle here)
+    if ((rc = copy_grid(ctx, h->x_e_box_prev, d.x_e_box_prev, bp, D2H, co))) return fail(rc);
+    if ((rc = copy_grid(ctx, h->x_e_box, d.x_e_box, bp, D2H, co))) return fail(rc);
+    if ((rc = copy_grid(ctx, h->Tk_box, d.Tk_box, br, D2H, co))) return fail(rc);
+    if ((rc = copy_grid(ctx, h->TS_box, d.TS_box, br, D2H, co))) return fail(rc);
+  } else {
+    if ((rc = hii_uploads())) return fail(rc);
+  }
+  // deltax and stars (and x_e_box, Tk_box from ComputeTs) are on the device already
+  hs.host_r_bubble = h->r_bubble;
+  if ((rc = find_hii(ctx, p, s, &d, hii_out, &hs))) return fail(rc);
+  if ((rc = copy_grid(ctx, h->xH, d.xH, br, D2H, co))) return fail(rc);
+  if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H, co))) return fail(rc);
+  if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H, co))) return fail(rc);
+  if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H, co))) return fail(rc);
+  if (h->delta_T) {
+    rg_grids dd = d;
+    if (vel) dd.vel = ctx->vel_stage;
+    if ((rc = rg_delta_T(ctx, p, s, &dd, volume_ave_Tb))) return fail(rc);
+    if ((rc = copy_grid(ctx, h->delta_T, d.delta_T, br, D2H))) return fail(rc);
+  }
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(cs));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(co));
   return RG_OK;
 }
 

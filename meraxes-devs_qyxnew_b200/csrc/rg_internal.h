@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -100,6 +101,9 @@ struct Staging {
   cudaEvent_t closing = nullptr;   // find_HII: temperature, Tk_box, weighted_sfr, effective_bhar
                                    // (closing pass); Ts: Tk_box (the evolution step)
   float* host_r_bubble = nullptr;  // find_HII: copy r_bubble here on the copy stream once zeroed
+  // ComputeTs: called once all of its own copies are queued and before the host first waits
+  // for the device, so a caller can queue the next step's copies behind them
+  std::function<int()> after_sources;
 };
 int stage_wait(rg_context* ctx, cudaEvent_t ev, cudaStream_t st);
 // record event i of the context's staging pool on st (events 0-3 are used by the host entry
@@ -196,6 +200,7 @@ struct rg_context {
   int num_sms = 0;
   // host entry points: uploads and early downloads run on copy_stream, ordered by these events
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t copy_stream_out = nullptr;   // device-to-host copies that overlap later work
   std::vector<cudaEvent_t> stage_events;
   // profiling
   bool prof_on = false;

@@ -675,6 +675,12 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   int rc;
   const Staging none;
   if (!stg) stg = &none;
+  bool kicked = false;
+  auto kick = [&]() -> int {
+    if (kicked || !stg->after_sources) return RG_OK;
+    kicked = true;
+    return stg->after_sources();
+  };
   cudaStream_t st = ctx->stream;
   const int N = ctx->N;
   const size_t n3 = (size_t)N * N * N;
@@ -731,6 +737,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double ftpr3 = (4.0 / 3.0) * M_PI * std::pow(R0, 3.0) / pixel_volume;
 
   auto finish = [&](bool homog, int nblocks) -> int {
+    if ((rc = kick())) return rc;
     if ((rc = reduce_partials(ctx, partials, nblocks, TS_NSUM, ctx->d_sums, st))) return rc;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * TS_NSUM, cudaMemcpyDeviceToHost, st));
     int nonconv = 0;
@@ -887,6 +894,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, wcut, st)))
         return rc;
     }
+    if ((rc = kick())) return rc;
     // the frequency tables on the host while the device runs the transforms above
     TsTables tb;
     std::string msg;

@@ -115,6 +115,8 @@ _SIGS = {
     "rg_compute_Ts_host": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_snapshot), _P(rg_grids), _P(rg_ts_scalars)]),
     "rg_delta_T_host": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_snapshot), _P(rg_grids), _P(C.c_double)]),
     "rg_debug_filter_roundtrip": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_void_p, C.c_double, C.c_int]),
+    "rg_reion_step_host": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_snapshot), _P(rg_grids), _P(rg_ts_scalars),
+                                     _P(rg_hii_scalars), _P(C.c_double)]),
     "rg_power_spectrum_length": (C.c_int, [_P(rg_params), _P(C.c_int)]),
     "rg_power_spectrum": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_int, _P(C.c_float), _P(C.c_float),
                                     _P(C.c_float), _P(C.c_int)]),
