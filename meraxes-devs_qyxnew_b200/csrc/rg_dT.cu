@@ -155,6 +155,9 @@ __global__ void __launch_bounds__(DT_NT) k_rsd(float* __restrict__ dT, const flo
   auto wrap = [n](int k) { return ((k % n) + n) % n; };   // the reference's periodic index
   const double w_sub = c.sub_w / c.cell;
   const double half = (c.sub_w / 2.) / c.cell;
+  // the reference divides by the cell and sub-cell widths in every sub-cell; multiplying by the
+  // reciprocals instead moves positions and shares by at most an ulp of double
+  const double inv_cell = 1.0 / c.cell, inv_w_sub = 1.0 / w_sub;
   for (int kk = threadIdx.x; kk < n; kk += DT_NT) {
     const float d = dT[row * n + kk];
     if (!(fabs((double)d) >= FRACT_FLOAT_ERR && (double)xH[row * n + kk] >= FRACT_FLOAT_ERR)) continue;
@@ -163,12 +166,13 @@ __global__ void __launch_bounds__(DT_NT) k_rsd(float* __restrict__ dT, const flo
     const double d1_high = (double)(v[kk] / c.H_z);
     const double d2_high = (double)(v[kk == n - 1 ? 0 : kk + 1] / c.H_z);
     const float val = d / (float)N_RSD_STEPS;
-    auto put = [&](int k, double frac) { atomicAdd(acc + wrap(k), (float)(frac * (double)d / (double)N_RSD_STEPS)); };
+    const double dd = (double)d / (double)N_RSD_STEPS;
+    auto put = [&](int k, double frac) { atomicAdd(acc + wrap(k), (float)(frac * dd)); };
     for (int s = 0; s < N_RSD_STEPS; ++s) {
       const double xp = (double)c.x_pos[s];
       const double disp = xp <= 0.5 ? d1_low + ((xp + 0.5) - 0.) * (d2_low - d1_low) / (1. - 0.)
                                     : d1_high + ((xp - 0.5) - 0.) * (d2_high - d1_high) / (1. - 0.);
-      const double pos = ((double)c.x_pos_offset[s] + disp) / c.cell;
+      const double pos = ((double)c.x_pos_offset[s] + disp) * inv_cell;
       const double lo = pos - half, hi = pos + half;
       if (lo >= 0.0 && hi < 1.0) {
         atomicAdd(acc + kk, val);
@@ -178,16 +182,16 @@ __global__ void __launch_bounds__(DT_NT) k_rsd(float* __restrict__ dT, const flo
         if (fabs(hi) > cd) {
           atomicAdd(acc + wrap(kk - (ic + 1)), val);
         } else {
-          const double fo = (fabs(lo) - cd) / w_sub, fw = 1. - fo;
+          const double fo = (fabs(lo) - cd) * inv_w_sub, fw = 1. - fo;
           put(kk - ic, fw);
           put(kk - (ic + 1), fo);
         }
       } else if (lo < 0.0 && (hi > 0.0 && hi < 1.0)) {
-        const double fw = hi / w_sub, fo = 1. - fw;
+        const double fw = hi * inv_w_sub, fo = 1. - fw;
         put(kk - 1, fo);
         put(kk, fw);
       } else if ((lo >= 0.0 && lo < 1.0) && (hi >= 1.0)) {
-        const double fo = (hi - 1.) / w_sub, fw = 1. - fo;
+        const double fo = (hi - 1.) * inv_w_sub, fw = 1. - fo;
         put(kk, fw);
         put(kk + 1, fo);
       } else {
@@ -196,7 +200,7 @@ __global__ void __launch_bounds__(DT_NT) k_rsd(float* __restrict__ dT, const flo
         if (lo >= cd) {
           atomicAdd(acc + wrap(kk + ic), val);
         } else {
-          const double fo = (hi - cd) / w_sub, fw = 1. - fo;
+          const double fo = (hi - cd) * inv_w_sub, fw = 1. - fo;
           put(kk + ic - 1, fw);
           put(kk + ic, fo);
         }
