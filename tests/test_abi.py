@@ -95,3 +95,16 @@ def test_create_without_device_reports_nodev():
     lib = rg.load()
     h = C.c_void_p()
     assert lib.rg_create(0, 64, C.byref(h)) == rg.RG_ENODEV
+
+
+def test_host_only_functions_reject_bad_arguments():
+    lib = rg.load()
+    n = C.c_int()
+    p = rg.make_params(32, 32.0)
+    assert lib.rg_power_spectrum_length(None, C.byref(n)) == rg.RG_EINVAL
+    bad = rg.make_params(32, -1.0)
+    assert lib.rg_power_spectrum_length(C.byref(bad), C.byref(n)) == rg.RG_EINVAL
+    assert lib.rg_power_spectrum_length(C.byref(p), C.byref(n)) == rg.RG_OK and n.value > 0
+    radii = (C.c_double * 8)()
+    assert lib.rg_radius_schedule(C.byref(bad), 8.0, radii, 8, C.byref(n)) == rg.RG_EINVAL
+    assert lib.rg_params_default(None, 32, 32.0) == rg.RG_EINVAL

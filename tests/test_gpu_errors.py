@@ -1,0 +1,96 @@
+"""Status codes of the C ABI on a GPU: invalid arguments and unimplemented configurations return
+RG_EINVAL / RG_EUNSUPPORTED with a message (the reference aborts the run instead), nothing is
+launched for them, and the context stays usable afterwards."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import rg_b200 as rg
+import workloads as wl
+from helpers import DeviceGrids
+
+pytestmark = pytest.mark.gpu
+
+
+def status(ctx, name, *args):
+    return getattr(ctx.lib, name)(ctx.h, *args)
+
+
+def test_unsupported_grid_dim_creates_no_context():
+    lib = rg.load()
+    h = C.c_void_p()
+    assert lib.rg_create(0, 40, C.byref(h)) == rg.RG_EUNSUPPORTED
+    assert not h.value
+
+
+def test_find_hii_rejections_leave_context_usable():
+    n = 16
+    src = wl.make_sources(n, 20.0, seed=1)
+    dg = DeviceGrids(n)
+    dg.put("deltax", src.deltax)
+    dg.put("stars", src.stars)
+    dg.put("weighted_sfr", src.sfr)
+    zz, snap = wl.snapshot_redshifts(8.0)
+    ctx = rg.Context(n)
+    out = rg.rg_hii_scalars()
+
+    def run(p, s=None, g=None):
+        s = s or rg.snapshot(zz, snap)
+        return status(ctx, "rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(g or dg.g), C.byref(out))
+
+    base = dict(Flag_EvolvingReionRBubbleMax=0, ReionRBubbleMax=20.0, ReionEfficiency=2000.0)
+    assert run(rg.make_params(32, 20.0, **base)) == rg.RG_EINVAL                       # N differs
+    assert "ReionGridDim" in ctx.lib.rg_last_error(ctx.h).decode()
+    assert run(rg.make_params(n, 20.0, Flag_IncludeRecombinations=1, **base)) == rg.RG_EUNSUPPORTED
+    assert run(rg.make_params(n, 20.0, ReionFilterType=3, **base)) == rg.RG_EINVAL
+    assert run(rg.make_params(n, 20.0, ReionDeltaRFactor=1.0, **base)) == rg.RG_EINVAL
+    assert run(rg.make_params(n, 20.0, **base), s=rg.snapshot(zz, len(zz) + 3)) == rg.RG_EINVAL
+    g = rg.rg_grids.from_buffer_copy(dg.g)
+    g.xH = None
+    assert run(rg.make_params(n, 20.0, **base), g=g) == rg.RG_EINVAL
+    assert run(rg.make_params(n, 20.0, Flag_IncludeSpinTemp=1, **base)) == rg.RG_EINVAL   # no x_e_box
+    # the context still works
+    assert run(rg.make_params(n, 20.0, **base)) == rg.RG_OK
+    assert 0.0 < out.volume_weighted_global_xH <= 1.0
+    ctx.close()
+
+
+def test_compute_ts_rejections():
+    for n, kw, code in ((48, {}, rg.RG_EUNSUPPORTED), (16, {"Flag_IncludeAGNXray": 1}, rg.RG_EUNSUPPORTED),
+                        (16, {"TsNumFilterSteps": 0}, rg.RG_EINVAL), (16, {"TsHeatingFilterType": 5}, rg.RG_EINVAL)):
+        dg = DeviceGrids(n, spin=True)
+        p = rg.make_params(n, 32.0, Flag_IncludeSpinTemp=1, **kw)
+        zz, snap = wl.snapshot_redshifts(15.0)
+        s = rg.snapshot(zz, snap, np.zeros(len(zz)))
+        ctx = rg.Context(n)
+        out = rg.rg_ts_scalars()
+        assert status(ctx, "rg_compute_Ts", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out)) == code, (n, kw)
+        ctx.close()
+
+
+def test_delta_T_and_power_spectrum_rejections():
+    import torch
+    n = 16
+    dg = DeviceGrids(n, spin=True)
+    zz, snap = wl.snapshot_redshifts(8.0)
+    s = rg.snapshot(zz, snap)
+    ctx = rg.Context(n)
+    tb = C.c_double()
+    p = rg.make_params(n, 20.0, Flag_IncludeSpinTemp=1, Flag_IncludePecVelsFor21cm=5)
+    assert status(ctx, "rg_delta_T", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(tb)) == rg.RG_EINVAL
+    p = rg.make_params(n, 20.0, Flag_IncludeSpinTemp=1, Flag_IncludePecVelsFor21cm=3)
+    assert status(ctx, "rg_delta_T", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(tb)) == rg.RG_EINVAL  # no vel
+    p = rg.make_params(n, 20.0)
+    d = torch.rand(n ** 3, device="cuda") + 1.0
+    k = (C.c_float * 2)()
+    nb = C.c_int()
+    rc = status(ctx, "rg_power_spectrum", C.byref(p), C.c_void_p(d.data_ptr()), 2, k, k, k, C.byref(nb))
+    assert rc == rg.RG_EINVAL and nb.value == rg.power_spectrum_length(p)
+    assert status(ctx, "rg_smooth_grid", C.c_double(-1.0), 8, C.c_void_p(d.data_ptr()),
+                  C.c_void_p(d.data_ptr())) == rg.RG_EINVAL
+    # still usable
+    kk, ps, err = ctx.power_spectrum(p, d.data_ptr())
+    assert len(kk) == nb.value
+    ctx.close()

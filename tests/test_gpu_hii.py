@@ -71,11 +71,12 @@ def run_gpu_hii(n, box, z, src, eff, ftype=0, mode=rg.RG_MODE_FUSED, state=None,
     return dg, out, p
 
 
-def check_against_oracle(n, box, z, src, eff, ftype, dg, out, p):
+def check_against_oracle(n, box, z, src, eff, ftype, dg, out, p, bh=None):
     op = oracle_params(p)
     st = ro.HIIState.fresh(n)
+    kw = {} if bh is None else {"effective_bhm": bh[0], "effective_bhar": bh[1]}
     xH_o, rb_o, s_o, diag = ro.find_hii_bubbles(op, z, src.deltax, src.stars, src.sfr, st, "fp64",
-                                                record_margins=True)
+                                                record_margins=True, **kw)
     xH = dg.get("xH")
     ion_g = xH < ro.REL_TOL
     ion_o = xH_o < ro.REL_TOL
@@ -103,8 +104,38 @@ def check_against_oracle(n, box, z, src, eff, ftype, dg, out, p):
               "mass_weighted_global_temp_kinetic_all_gas"):
         assert getattr(out, k) == pytest.approx(s_o[k], rel=1e-5), k
     assert abs(out.mass_weighted_global_xH - s_o["mass_weighted_global_xH"]) <= 1e-4
+    if bh is not None:
+        assert out.volume_weighted_global_effective_bhar == pytest.approx(
+            s_o["volume_weighted_global_effective_bhar"], rel=1e-5)
     assert out.n_radii == diag["n_radii"]
     return dis.sum()
+
+
+@pytest.mark.parametrize("n,box", [(32, 32.0), (64, 64.0)])
+def test_find_hii_bubbles_bh_feedback(n, box):
+    """Flag_BHFeedback: effective_bhm is a fourth filtered field in the barrier test (and in J_21);
+    effective_bhar enters the closing-pass average."""
+    z = 8.0
+    src = wl.make_sources(n, box, seed=31)
+    rng = np.random.default_rng(32)
+    bhm = (src.stars * 0.05 * rng.random(src.stars.shape)).astype(np.float32)
+    bhar = (bhm * 1e-3).astype(np.float32)
+    dg = DeviceGrids(n, bh=True)
+    dg.put("deltax", src.deltax)
+    dg.put("stars", src.stars)
+    dg.put("weighted_sfr", src.sfr)
+    dg.put("effective_bhm", bhm)
+    dg.put("effective_bhar", bhar)
+    p = rg.make_params(n, box, Flag_EvolvingReionRBubbleMax=0, ReionRBubbleMax=50.0, ReionEfficiency=3000.0,
+                       Flag_BHFeedback=1)
+    zz, snap = wl.snapshot_redshifts(z)
+    s = rg.snapshot(zz, snap)
+    ctx = rg.Context(n)
+    out = rg.rg_hii_scalars()
+    ctx.call("rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out))
+    ctx.close()
+    check_against_oracle(n, box, z, src, 3000.0, 0, dg, out, p, bh=(bhm, bhar))
+    assert 0.0 < out.volume_weighted_global_xH < 1.0
 
 
 @pytest.mark.parametrize("n,box,z,ftype", [(32, 32.0, 8.0, 0), (64, 64.0, 8.0, 0), (64, 64.0, 8.0, 1),
