@@ -614,7 +614,7 @@ def run_ours(args, cfg):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "ms/snapshot", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, BASELINE shapes)",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators at the workload's shapes and sizes)",
                 "config": dict(workload_desc(cfg, nr), mode=args.mode, parallelism=f"replicas x{ws}"),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clk, "results": results, "extras": extras}
@@ -769,7 +769,7 @@ def run_batch(args):
         value = len(units) / (ms_batch * 1e-3)
         line = {"metric": BATCH_METRIC, "value": value, "unit": "snapshots/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "strong",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, BASELINE shapes)",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators at the workload's shapes and sizes)",
                 "config": {"workload": "48 independent find_HII_bubbles snapshots, z = 16 -> 6, boxes 64^3, 96^3, "
                                        "128^3, 192^3 (12 each, L = N Mpc/h), efficiency calibrated for <xH> 0.99 -> 0.1",
                            "name": "c2_batch", "parallelism": f"units placed whole on {ws} rank(s)",
