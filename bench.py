@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--config", default=DEFAULT_CONFIG)
     ap.add_argument("--mode", default="fused", choices=["fused", "plain"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the timings reported under extras")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -564,10 +565,18 @@ def run_ours(args, cfg):
                                         "GBps": k["alg_bytes_total"] / max(k["ms_total"], 1e-9) / 1e6}
                             for k in stats}}
 
+    # the same step in the plain mode (one FFT chain per grid per radius, the reference's pass
+    # structure, every grid it filters): the baseline of the fused mode
+    extras = {}
+    if args.mode == "fused" and not args.no_extras:
+        ctx.call("rg_set_mode", rg.RG_MODE_PLAIN)
+        tp = timed(torch, stream, wk.step, wk.reset, 2, max(2, min(args.steps, 3)))
+        ctx.call("rg_set_mode", rg.RG_MODE_FUSED)
+        extras["plain_mode"] = {"ms_per_step": statistics.mean(tp),
+                                "what": "the step with RG_MODE_PLAIN (unbatched radii, separate passes)"}
     # the 21-cm power spectrum of the step's delta_T (Compute_PS, run after the step by the
     # reference when Flag_ComputePS is set): not part of the metric, timed on its own
-    extras = {}
-    if wk.spin:
+    if wk.spin and not args.no_extras:
         dptr = wk.b["delta_T"].data_ptr()
         ctx.power_spectrum(wk.p, dptr)
         torch.cuda.synchronize(dev)
