@@ -753,14 +753,7 @@ int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   // the velocity grid of delta_T's velocity modes goes to its own device buffer
   const bool vel = h->delta_T && spin && p->Flag_IncludePecVelsFor21cm > 0;
   if (vel && !h->vel) return set_error(ctx, RG_EINVAL, "missing grid pointer");
-  if (vel && (!ctx->vel_stage || ctx->vel_stage_elems < bp / sizeof(float))) {
-    if (ctx->vel_stage) cudaFree(ctx->vel_stage);
-    ctx->vel_stage = nullptr;
-    ctx->vel_stage_elems = 0;
-    if (cudaMalloc((void**)&ctx->vel_stage, bp) != cudaSuccess)
-      return set_error(ctx, RG_ENOMEM, "cudaMalloc of the velocity grid");
-    ctx->vel_stage_elems = bp / sizeof(float);
-  }
+  if (vel && (rc = ensure_device(ctx, &ctx->vel_stage, &ctx->vel_stage_elems, bp / sizeof(float)))) return rc;
   if ((rc = copy_stream_after_prior(ctx))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamWaitEvent(co, ctx->stage_events[0], 0));
   Staging hs;   // find_HII's copies

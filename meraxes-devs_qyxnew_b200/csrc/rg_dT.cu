@@ -231,22 +231,8 @@ static int velocity_modes(rg_context* ctx, const rg_params* p, const rg_grids* g
   const int flag = p->Flag_IncludePecVelsFor21cm;
   const size_t nc = (size_t)(n / 2 + 1) * n * n, npad = 2 * nc, n3 = (size_t)n * n * n;
   int rc;
-  if (!ctx->vel_work || ctx->vel_work_elems < 2 * npad) {
-    if (ctx->vel_work) cudaFree(ctx->vel_work);
-    ctx->vel_work = nullptr;
-    ctx->vel_work_elems = 0;
-    if (cudaMalloc((void**)&ctx->vel_work, sizeof(float) * 2 * npad) != cudaSuccess)
-      return set_error(ctx, RG_ENOMEM, "cudaMalloc of the velocity work grids");
-    ctx->vel_work_elems = 2 * npad;
-  }
-  if (!ctx->spec || ctx->spec_elems < nc) {
-    if (ctx->spec) cudaFree(ctx->spec);
-    ctx->spec = nullptr;
-    ctx->spec_elems = 0;
-    if (cudaMalloc((void**)&ctx->spec, sizeof(cf) * nc) != cudaSuccess)
-      return set_error(ctx, RG_ENOMEM, "cudaMalloc of the velocity spectrum");
-    ctx->spec_elems = nc;
-  }
+  if ((rc = ensure_device(ctx, &ctx->vel_work, &ctx->vel_work_elems, 2 * npad))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc))) return rc;
   float* vc = ctx->vel_work;
   float* grad = ctx->vel_work + npad;
   const Cosmo cm(p);
@@ -356,14 +342,8 @@ int rg_delta_T_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, c
   rg_grids dv = d;
   if (p->Flag_IncludeSpinTemp && p->Flag_IncludePecVelsFor21cm > 0) {
     if (!h->vel) return set_error(ctx, RG_EINVAL, "missing grid pointer");
-    if (!ctx->vel_stage || ctx->vel_stage_elems < bp / sizeof(float)) {
-      if (ctx->vel_stage) cudaFree(ctx->vel_stage);
-      ctx->vel_stage = nullptr;
-      ctx->vel_stage_elems = 0;
-      if (cudaMalloc((void**)&ctx->vel_stage, bp) != cudaSuccess)
-        return set_error(ctx, RG_ENOMEM, "cudaMalloc of the velocity grid");
-      ctx->vel_stage_elems = bp / sizeof(float);
-    }
+    int rv = ensure_device(ctx, &ctx->vel_stage, &ctx->vel_stage_elems, bp / sizeof(float));
+    if (rv) return rv;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->vel_stage, h->vel, bp, cudaMemcpyHostToDevice, st));
     dv.vel = ctx->vel_stage;
   }

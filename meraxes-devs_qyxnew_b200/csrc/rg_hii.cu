@@ -651,15 +651,8 @@ int reduce_partials(rg_context* ctx, const double* partials, int nblocks, int ns
 }
 
 int xy_ctrl_reset(rg_context* ctx, size_t max_jobs, cudaStream_t st) {
-  const size_t need = max_jobs + 2;
-  if (!ctx->xy_ctrl || ctx->xy_ctrl_elems < need) {
-    if (ctx->xy_ctrl) cudaFree(ctx->xy_ctrl);
-    ctx->xy_ctrl = nullptr;
-    ctx->xy_ctrl_elems = 0;
-    cudaError_t e = cudaMalloc((void**)&ctx->xy_ctrl, sizeof(uint32_t) * need);
-    if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    ctx->xy_ctrl_elems = need;
-  }
+  int rc = ensure_device(ctx, &ctx->xy_ctrl, &ctx->xy_ctrl_elems, max_jobs + 2);
+  if (rc) return rc;
   RG_CUDA_TRY(ctx, cudaMemsetAsync(ctx->xy_ctrl, 0, sizeof(uint32_t), st));
   return RG_OK;
 }
@@ -670,18 +663,6 @@ int xy_ctrl_check(rg_context* ctx, cudaStream_t st) {
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(&err, ctx->xy_ctrl, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (err) return set_error(ctx, RG_ETIMEDOUT, "fused x/y pass: a wait for the x pass of a plane ran out");
-  return RG_OK;
-}
-
-template <typename T>
-static int ensure_buf(rg_context* ctx, T** ptr, size_t* have, size_t need) {
-  if (*ptr && *have >= need) return RG_OK;
-  if (*ptr) cudaFree(*ptr);
-  *ptr = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * need);
-  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  *have = need;
   return RG_OK;
 }
 
@@ -730,10 +711,10 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   int kb = plain ? 1 : (ctx->radius_batch > 0 ? ctx->radius_batch : 8);
   if (kb > KB_MAX) kb = KB_MAX;
   if (kb > nr) kb = nr;
-  if ((rc = ensure_buf(ctx, &ctx->spec, &ctx->spec_elems, nc * ng))) return rc;
-  if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc * ng * kb))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * ng))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * ng * kb))) return rc;
   const size_t nw = bit_words(N);
-  if ((rc = ensure_buf(ctx, &ctx->bits, &ctx->bits_elems, 2 * nw))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->bits, &ctx->bits_elems, 2 * nw))) return rc;
   if ((rc = stage_wait(ctx, stg->inputs, st))) return rc;
   if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
 
@@ -741,10 +722,10 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   const int n2max = 3 * (N / 2) * (N / 2);
   std::vector<double> radii(nr);
   for (int i = 0; i < nr; ++i) radii[i] = sched[i].first;
-  if ((rc = ensure_buf(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
-  if ((rc = ensure_buf(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
-  if ((rc = ensure_buf(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nr))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nr))) return rc;
   if ((rc = window_table(ctx, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st, ctx->wcut)))
     return rc;
   const int* wcut = p->ReionFilterType == 1 ? ctx->wcut : nullptr;
@@ -834,7 +815,7 @@ static int debug_inverse(rg_context* ctx, int n, const float* wrow, float* d_out
 int spectrum_to_padded(rg_context* ctx, float* d_out, cudaStream_t st) {
   const size_t nc = (size_t)(ctx->N / 2 + 1) * ctx->N * ctx->N;
   int rc;
-  if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc))) return rc;
   return debug_inverse(ctx, ctx->N, nullptr, d_out, st);
 }
 
@@ -843,16 +824,16 @@ int debug_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in, floa
   cudaStream_t st = ctx->stream;
   const int N = ctx->N;
   const size_t nc = (size_t)(N / 2 + 1) * N * N;
-  if ((rc = ensure_buf(ctx, &ctx->spec, &ctx->spec_elems, nc))) return rc;
-  if ((rc = ensure_buf(ctx, &ctx->work, &ctx->work_elems, nc))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc))) return rc;
   const float* srcs[1] = {d_in};
   if ((rc = fft_forward(ctx, N, srcs, 1, ctx->spec, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
   const float* wrow = nullptr;
   if (ftype >= 0) {
     const int n2max = 3 * (N / 2) * (N / 2);
-    if ((rc = ensure_buf(ctx, &ctx->d_radii, &ctx->d_radii_elems, 1))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->d_radii, &ctx->d_radii_elems, 1))) return rc;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, &R, sizeof(double), cudaMemcpyHostToDevice, st));
-    if ((rc = ensure_buf(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)(n2max + 1)))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)(n2max + 1)))) return rc;
     if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, 1, ftype, ctx->wtab, n2max, st))) return rc;
     wrow = ctx->wtab;
   }

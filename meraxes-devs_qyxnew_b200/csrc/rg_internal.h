@@ -76,6 +76,20 @@ int set_error(rg_context* ctx, int status, const std::string& msg);
       return ::rg::set_error((ctx), RG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// A context buffer of at least `need` elements: kept when large enough, else freed and allocated
+// again (the old contents are not kept).
+template <typename T>
+int ensure_device(rg_context* ctx, T** ptr, size_t* have, size_t need) {
+  if (*ptr && *have >= need) return RG_OK;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *have = 0;
+  const cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * (need ? need : 1));
+  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  *have = need;
+  return RG_OK;
+}
+
 // Per-snapshot constants of the barrier test.
 struct HiiConst {
   float redshift, TK, cT_ad;

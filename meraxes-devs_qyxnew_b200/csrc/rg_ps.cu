@@ -161,18 +161,6 @@ __global__ void __launch_bounds__(PS_NT) k_ps_bins(const cf* __restrict__ spec, 
   }
 }
 
-template <typename T>
-static int ps_ensure(rg_context* ctx, T** ptr, size_t* have, size_t need) {
-  if (*ptr && *have >= need) return RG_OK;
-  if (*ptr) cudaFree(*ptr);
-  *ptr = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * need);
-  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  *have = need;
-  return RG_OK;
-}
-
 static int power_spectrum(rg_context* ctx, const rg_params* p, const float* d_dT, int max_bins, float* PS_k,
                           float* PS_data, float* PS_error, int* n_bins) {
   int rc = validate_common(ctx, p);
@@ -185,8 +173,8 @@ static int power_spectrum(rg_context* ctx, const rg_params* p, const float* d_dT
   cudaStream_t st = ctx->stream;
   const int N = ctx->N;
   const size_t n3 = (size_t)N * N * N, nc = (size_t)(N / 2 + 1) * N * N, npad = 2 * nc;
-  if ((rc = ps_ensure(ctx, &ctx->spec, &ctx->spec_elems, nc))) return rc;
-  if ((rc = ps_ensure(ctx, &ctx->ps_pad, &ctx->ps_pad_elems, npad))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->ps_pad, &ctx->ps_pad_elems, npad))) return rc;
   const int nblk = 4 * ctx->num_sms;
   double* partials = ensure_partials(ctx, (size_t)nblk * 3 * PS_MAXBINS);
   if (!partials) return set_error(ctx, RG_ENOMEM, "partials");
@@ -254,7 +242,7 @@ int rg_power_spectrum_host(rg_context* ctx, const rg_params* p, const float* h_d
   if (rc) return rc;
   cudaSetDevice(ctx->device);
   const size_t n3 = (size_t)ctx->N * ctx->N * ctx->N;
-  if ((rc = ps_ensure(ctx, &ctx->ps_stage, &ctx->ps_stage_elems, n3))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->ps_stage, &ctx->ps_stage_elems, n3))) return rc;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ps_stage, h_delta_T, sizeof(float) * n3, cudaMemcpyHostToDevice, ctx->stream));
   return power_spectrum(ctx, p, ctx->ps_stage, max_bins, PS_k, PS_data, PS_error, n_bins);
 }

@@ -586,18 +586,6 @@ static void fill_spline(const CubicSpline& sp, const std::vector<double>& lx, co
   }
 }
 
-template <typename T>
-static int ensure_mem(rg_context* ctx, T** ptr, size_t* have, size_t need) {
-  if (*ptr && *have >= need) return RG_OK;
-  if (*ptr) cudaFree(*ptr);
-  *ptr = nullptr;
-  *have = 0;
-  cudaError_t e = cudaMalloc((void**)ptr, sizeof(T) * need);
-  if (e != cudaSuccess) return set_error(ctx, RG_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  *have = need;
-  return RG_OK;
-}
-
 // x and y passes of a batch of shells: work_base + (j * 2 + g) * stride, j < bt.nr
 template <int N>
 static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
@@ -721,7 +709,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   // context buffer: [TsDev][int + pad][TsShellCoef x shells]
   const int nS_all = p->TsNumFilterSteps;
   const size_t off_co = (sizeof(TsDev) + 16 + 255) / 256 * 256;
-  if ((rc = ensure_mem(ctx, &ctx->ts_const, &ctx->ts_const_elems, off_co + sizeof(TsShellCoef) * (nS_all + 1))))
+  if ((rc = ensure_device(ctx, &ctx->ts_const, &ctx->ts_const_elems, off_co + sizeof(TsShellCoef) * (nS_all + 1))))
     return rc;
   TsDev* d_hc = reinterpret_cast<TsDev*>(ctx->ts_const);
   int* d_nonconv = reinterpret_cast<int*>(ctx->ts_const + sizeof(TsDev));
@@ -817,25 +805,25 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       if (nk > TS_MAXSRC) return set_error(ctx, RG_EUNSUPPORTED, "a shell combines more than 4 history snapshots");
     }
     const int nused = std::max(1, (int)used.size());
-    if ((rc = ensure_mem(ctx, &ctx->spec, &ctx->spec_elems, nc * 2 * nused))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * 2 * nused))) return rc;
     // every shell's filtered grids stay in HBM until the fused z pass (2 nS spectra)
-    if ((rc = ensure_mem(ctx, &ctx->work, &ctx->work_elems, nc * 2 * nS))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * 2 * nS))) return rc;
     // source grid `which` (0 sfr, 1 xray) of source k, on the device
     const rg_grids* sg = src_host ? src_host : g;
     auto src_grid = [&](int k, int which) -> const float* {
       if (k == 0) return which ? sg->xray_luminosity : sg->sfr;
       return (which ? sg->xray_luminosity_histories : sg->sfr_histories) + (size_t)(k - 1) * npad;
     };
-    if (src_host && (rc = ensure_mem(ctx, &ctx->ts_stage, &ctx->ts_stage_elems, npad * 2 * used.size()))) return rc;
+    if (src_host && (rc = ensure_device(ctx, &ctx->ts_stage, &ctx->ts_stage_elems, npad * 2 * used.size()))) return rc;
     auto dev_grid = [&](size_t j, int which) -> const float* {
       return src_host ? ctx->ts_stage + (j * 2 + which) * npad : src_grid(used[j], which);
     };
     // window rows for the shells (filter() takes BoxSize in Mpc/h and R in Mpc, ComputeTs.c:532)
     const int n2max = 3 * (N / 2) * (N / 2);
-    if ((rc = ensure_mem(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nS))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nS))) return rc;
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, sh.R.data(), sizeof(double) * nS, cudaMemcpyHostToDevice, st));
-    if ((rc = ensure_mem(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nS * (n2max + 1)))) return rc;
-    if ((rc = ensure_mem(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nS))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nS * (n2max + 1)))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nS))) return rc;
     if ((rc = window_table(ctx, p->BoxSize, ctx->d_radii, nS, p->TsHeatingFilterType, ctx->wtab, n2max, st,
                            ctx->wcut)))
       return rc;
@@ -950,7 +938,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     }
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(d_co, hco.data(), sizeof(TsShellCoef) * (nS + 1), cudaMemcpyHostToDevice, st));
     zv.nS = nS;
-    if ((rc = ensure_mem(ctx, &ctx->ts_sums, &ctx->ts_sums_elems, n3))) return rc;
+    if ((rc = ensure_device(ctx, &ctx->ts_sums, &ctx->ts_sums_elems, n3))) return rc;
     if ((rc = ts_zsum(ctx, N, ctx->work, nc, d_co, zv, g->x_e_box_prev, ctx->ts_sums, st))) return rc;
     RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // hco outlives the copy
   }
