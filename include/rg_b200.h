@@ -219,6 +219,17 @@ int rg_power_spectrum_host(rg_context* ctx, const rg_params* p, const float* h_d
 int rg_smooth_grid(rg_context* ctx, double box_size, int reion_grid_dim, const float* d_in_padded,
                    float* d_out_padded);
 
+/* The nearest-grid-point deposit of construct_baryon_grids (src/core/reionization.c:2025-2592)
+   for one rank holding the whole grid: galaxy g at d_pos[3g .. 3g+2] (box units, [0, box_size))
+   adds d_values[p * n_gal + g] to grid p at the cell pos_to_ngp (src/core/misc_tools.c:207-217)
+   gives; each grid is then clamped at zero, divided by divisors[p] (a host array, or null for
+   none; the sfr grid's SFR timescale) and left in the padded layout.  The grids are overwritten
+   (device pointers, n_prop <= 8).  Which galaxy property goes to which grid, the black-hole mass
+   limit and the history shift stay with the caller.  A position below the box returns RG_EINVAL
+   (the reference asserts). */
+int rg_deposit_ngp(rg_context* ctx, double box_size, int n_gal, const float* d_pos, int n_prop,
+                   const float* d_values, const double* divisors, float* const* d_grids);
+
 /* ---- per-kernel timing: CUDA events on the launching stream around every launch ---- */
 typedef struct rg_kernel_stat {
   char name[48];

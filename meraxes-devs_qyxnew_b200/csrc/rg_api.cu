@@ -319,6 +319,7 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->ps_stage) cudaFree(ctx->ps_stage);
   if (ctx->vel_work) cudaFree(ctx->vel_work);
   if (ctx->vel_stage) cudaFree(ctx->vel_stage);
+  if (ctx->ngp_bad) cudaFree(ctx->ngp_bad);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);

@@ -189,6 +189,8 @@ struct rg_context {
   size_t vel_work_elems = 0;
   float* vel_stage = nullptr;    // rg_delta_T_host: device copy of the caller's velocity grid
   size_t vel_stage_elems = 0;
+  int* ngp_bad = nullptr;        // rg_deposit_ngp: count of galaxies below the box
+  size_t ngp_bad_elems = 0;
   double* partials = nullptr;
   size_t partials_elems = 0;
   double* d_sums = nullptr;      // reduced sums

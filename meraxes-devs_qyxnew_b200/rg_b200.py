@@ -123,6 +123,8 @@ _SIGS = {
     "rg_power_spectrum_host": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_int, _P(C.c_float),
                                          _P(C.c_float), _P(C.c_float), _P(C.c_int)]),
     "rg_smooth_grid": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
+    "rg_deposit_ngp": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                 C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
     "rg_radius_schedule": (C.c_int, [_P(rg_params), C.c_double, _P(C.c_double), C.c_int, _P(C.c_int)]),
     "rg_debug_ts_tables": (C.c_int, [_P(rg_params), _P(rg_snapshot), C.c_int, C.c_double, C.c_double, C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -256,6 +258,15 @@ class Context:
         m = n.value
         return (np.frombuffer(k, np.float32)[:m].copy(), np.frombuffer(d, np.float32)[:m].copy(),
                 np.frombuffer(e, np.float32)[:m].copy())
+
+    def deposit_ngp(self, box_size: float, n_gal: int, pos_ptr: int, values_ptr: int, grid_ptrs, divisors=None):
+        """Nearest-grid-point deposit of n_gal galaxies (device positions [n_gal][3] and values
+        [n_prop][n_gal]) into the padded device grids grid_ptrs (overwritten)."""
+        n_prop = len(grid_ptrs)
+        grids = (C.c_void_p * n_prop)(*grid_ptrs)
+        div = (C.c_double * n_prop)(*divisors) if divisors is not None else None
+        self.call("rg_deposit_ngp", box_size, n_gal, C.c_void_p(pos_ptr), n_prop, C.c_void_p(values_ptr),
+                  div, grids)
 
     def profile(self, on: bool):
         self.call("rg_profile_enable", int(on))
