@@ -71,6 +71,9 @@ typedef struct rg_params {
   /* merger-tree code of the velocity grid (meraxes.h:253-258): 0 VELOCIraptor, 1 gbpTrees,
      2 VELOCIraptor (augmented); sets the units of rg_grids.vel */
   int TreesID;
+  /* recombinations (Flag_IncludeRecombinations): 1 = the MHR rates at the cell's gas
+     temperature, 0 = at 10^4 K (find_HII_bubbles.c:613-619) */
+  int Flag_TemperatureDependentRec;
 } rg_params;
 
 /* Fill *p with the values of input/params/defaults.par and the Genesis cosmology/units. */
@@ -109,6 +112,15 @@ typedef struct rg_grids {
      temperature when Flag_IncludePecVelsFor21cm > 0.  The reference converts this grid in
      place (BrightnessTemperature.c:173-196); the library leaves it unchanged. */
   const float* vel;
+  /* inhomogeneous recombinations (Flag_IncludeRecombinations), reionization.c:1266-1292:
+     N_rec padded and persistent (the cumulative recombinations per baryon); Gamma12 real and
+     persistent (the ionising background at the cell's first crossing, 1e-12 s^-1 h^-2);
+     residual_xH, clumping_factor and t_resp (Myr) real outputs */
+  float* Gamma12;
+  float* N_rec;
+  float* residual_xH;
+  float* clumping_factor;
+  float* t_resp;
 } rg_grids;
 
 /* The snapshot being processed: run_globals.ZZ[] and the snapshot index into it. */
@@ -131,6 +143,11 @@ typedef struct rg_hii_scalars {
   double mass_weighted_global_r_bubble;
   double mass_weighted_global_temp_kinetic_all_gas;
   int n_radii;                      /* filter radii processed */
+  /* Flag_IncludeRecombinations only (0 otherwise) */
+  double volume_weighted_global_Gamma12, volume_weighted_global_N_rec;
+  double volume_weighted_global_residual_xH, volume_weighted_global_clumping_factor;
+  double mass_weighted_global_Gamma12, mass_weighted_global_N_rec;
+  double mass_weighted_global_residual_xH, mass_weighted_global_clumping_factor;
 } rg_hii_scalars;
 
 typedef struct rg_ts_scalars {
@@ -161,10 +178,25 @@ int rg_alloc_grids(rg_context* ctx, const rg_params* p, int n_hist, rg_grids* ou
 /* init_reion_grids() (src/core/reionization.c:504-716) for the device grids. */
 int rg_init_reion_grids(rg_context* ctx, const rg_params* p, const rg_grids* g);
 
+/* The MHR00 recombination tables of init_MHR() (src/core/recombinations.c:208-373), which a
+   run with Flag_IncludeRecombinations must hand over once before its first find_HII_bubbles:
+   lnGamma[n_gamma] (the knots, ln Gamma12), and RR (ln of the recombination rate), CF (the
+   clumping factor) and RNH (ln of the residual neutral fraction), each [n_z][n_t][n_gamma]
+   as Meraxes holds RR_table / CF_table / RNH_table (recombinations.h:17-34: 200 redshifts
+   0, 0.2, ...; 100 temperatures log10 T = 2, 2.03, ...; 150 values of ln Gamma12).  The
+   natural cubic splines of splined_recombination() (recombinations.c:35-84) are set up here,
+   in FP64, and kept on the device; the host arrays may be freed on return. */
+int rg_set_recombination_tables(rg_context* ctx, const double* lnGamma, int n_z, int n_t, int n_gamma,
+                                const double* RR, const double* CF, const double* RNH);
+
 /* ---- the grid step (device pointers, asynchronous on the context stream; scalars
         are written before return, so these synchronise the stream once) ---- */
 
-/* _find_HII_bubbles (src/core/find_HII_bubbles.c:86-710). */
+/* _find_HII_bubbles (src/core/find_HII_bubbles.c:86-710).  With Flag_IncludeRecombinations
+   it also filters N_rec and weighted_sfr (and effective_bhar), tests the barrier against
+   1 + N_rec, records Gamma12, r_bubble (and J_21 for ReionUVBFlag 2) at each cell's first
+   crossing, and updates N_rec, residual_xH, clumping_factor and t_resp in the closing pass
+   (:226-230,467-508,613-644); rg_set_recombination_tables must have been called. */
 int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
                         rg_hii_scalars* out);
 /* _ComputeTs (src/core/ComputeTs.c:85-1554). */

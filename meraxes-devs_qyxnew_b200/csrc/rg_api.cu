@@ -2,6 +2,7 @@
 // grid step (find_HII_bubbles, ComputeTs, delta_T).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -267,6 +268,7 @@ int rg_params_default(rg_params* p, int grid_dim, double box_size) {
   p->NuXraySoftCut = 2000.;
   p->NuXrayMax = 10000.;
   p->SpecIndexXrayGal = 1.;
+  p->Flag_TemperatureDependentRec = 1;   // input/params/defaults.par:19
   return RG_OK;
 }
 
@@ -320,6 +322,9 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->vel_work) cudaFree(ctx->vel_work);
   if (ctx->vel_stage) cudaFree(ctx->vel_stage);
   if (ctx->ngp_bad) cudaFree(ctx->ngp_bad);
+  if (ctx->rec_knots) cudaFree(ctx->rec_knots);
+  if (ctx->rec_y) cudaFree(ctx->rec_y);
+  if (ctx->rec_c) cudaFree(ctx->rec_c);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
@@ -407,6 +412,13 @@ int rg_alloc_grids(rg_context* ctx, const rg_params* p, int n_hist, rg_grids* ou
   RG_ALLOC(temp_kinetic_all_gas, nreal);
   RG_ALLOC(delta_T, nreal);
   if (p->Flag_IncludeSpinTemp && p->Flag_IncludePecVelsFor21cm > 0) RG_ALLOC(vel, npad);
+  if (p->Flag_IncludeRecombinations) {
+    RG_ALLOC(Gamma12, nreal);
+    RG_ALLOC(N_rec, npad);
+    RG_ALLOC(residual_xH, nreal);
+    RG_ALLOC(clumping_factor, nreal);
+    RG_ALLOC(t_resp, nreal);
+  }
   if (p->Flag_IncludeSpinTemp) {
     RG_ALLOC(x_e_box_prev, npad);
     RG_ALLOC(x_e_box, npad);
@@ -442,6 +454,12 @@ int rg_init_reion_grids(rg_context* ctx, const rg_params* p, const rg_grids* g) 
   if ((rc = fill(ctx, g->TS_box, nreal, 0.f))) return rc;
   if ((rc = fill(ctx, g->x_e_box_prev, npad, 0.f))) return rc;
   if ((rc = fill(ctx, g->x_e_box, npad, 0.f))) return rc;
+  // reionization.c:576-582,698
+  if ((rc = fill(ctx, g->Gamma12, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->residual_xH, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->clumping_factor, nreal, 0.f))) return rc;
+  if ((rc = fill(ctx, g->t_resp, nreal, 1e30f))) return rc;
+  if ((rc = fill(ctx, g->N_rec, npad, 0.f))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }
@@ -453,8 +471,12 @@ static int find_hii(rg_context* ctx, const rg_params* p, const rg_snapshot* s, c
   int rc = validate_common(ctx, p);
   if (rc) return rc;
   if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return set_error(ctx, RG_EINVAL, "snapshot out of range");
-  if (p->Flag_IncludeRecombinations)
-    return set_error(ctx, RG_EUNSUPPORTED, "Flag_IncludeRecombinations=1 (MHR00 recombination tables) is not implemented");
+  if (p->Flag_IncludeRecombinations) {
+    if (!ctx->rec_y)
+      return set_error(ctx, RG_EINVAL, "Flag_IncludeRecombinations needs rg_set_recombination_tables first");
+    if (!g->Gamma12 || !g->N_rec || !g->residual_xH || !g->clumping_factor || !g->t_resp)
+      return set_error(ctx, RG_EINVAL, "recombinations need Gamma12, N_rec, residual_xH, clumping_factor, t_resp");
+  }
   if (p->ReionFilterType < 0 || p->ReionFilterType > 2)
     return set_error(ctx, RG_EINVAL, "ReionFilterType must be 0, 1 or 2");
   if (p->ReionRtoMFilterType < 0 || p->ReionRtoMFilterType > 1)
@@ -507,6 +529,50 @@ static int copy_stream_after_prior(rg_context* ctx) {
 
 extern "C" {
 
+int rg_set_recombination_tables(rg_context* ctx, const double* lnGamma, int n_z, int n_t, int n_gamma,
+                                const double* RR, const double* CF, const double* RNH) {
+  if (!ctx || !lnGamma || !RR || !CF || !RNH || n_z < 1 || n_t < 1 || n_gamma < 3) return RG_EINVAL;
+  for (int i = 0; i + 1 < n_gamma; ++i)
+    if (!(lnGamma[i + 1] > lnGamma[i])) return set_error(ctx, RG_EINVAL, "lnGamma knots must increase");
+  cudaSetDevice(ctx->device);
+  const size_t rows = (size_t)n_z * n_t, per = rows * (size_t)n_gamma;
+  // natural cubic spline of every (table, z, T) row in ln Gamma12 (init_MHR's gsl_interp_cspline
+  // splines, recombinations.c:347-363)
+  std::vector<double> c(3 * per);
+  const std::vector<double> x(lnGamma, lnGamma + n_gamma);
+  const double* tabs[3] = {RR, CF, RNH};
+  CubicSpline sp;
+  for (int k = 0; k < 3; ++k)
+    for (size_t r = 0; r < rows; ++r) {
+      const double* y = tabs[k] + r * n_gamma;
+      if (!sp.init(x, std::vector<double>(y, y + n_gamma)))
+        return set_error(ctx, RG_EINVAL, "recombination spline setup failed");
+      const std::vector<double>& h = sp.half_curvature();
+      std::copy(h.begin(), h.end(), c.begin() + ((size_t)k * rows + r) * n_gamma);
+    }
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->rec_knots) cudaFree(ctx->rec_knots);
+  if (ctx->rec_y) cudaFree(ctx->rec_y);
+  if (ctx->rec_c) cudaFree(ctx->rec_c);
+  ctx->rec_knots = ctx->rec_y = ctx->rec_c = nullptr;
+  if (cudaMalloc((void**)&ctx->rec_knots, sizeof(double) * n_gamma) != cudaSuccess ||
+      cudaMalloc((void**)&ctx->rec_y, sizeof(double) * 3 * per) != cudaSuccess ||
+      cudaMalloc((void**)&ctx->rec_c, sizeof(double) * 3 * per) != cudaSuccess) {
+    if (ctx->rec_knots) cudaFree(ctx->rec_knots);
+    if (ctx->rec_y) cudaFree(ctx->rec_y);
+    ctx->rec_knots = ctx->rec_y = ctx->rec_c = nullptr;
+    return set_error(ctx, RG_ENOMEM, "cudaMalloc of the recombination tables failed");
+  }
+  RG_CUDA_TRY(ctx, cudaMemcpy(ctx->rec_knots, lnGamma, sizeof(double) * n_gamma, cudaMemcpyHostToDevice));
+  for (int k = 0; k < 3; ++k)
+    RG_CUDA_TRY(ctx, cudaMemcpy(ctx->rec_y + (size_t)k * per, tabs[k], sizeof(double) * per, cudaMemcpyHostToDevice));
+  RG_CUDA_TRY(ctx, cudaMemcpy(ctx->rec_c, c.data(), sizeof(double) * 3 * per, cudaMemcpyHostToDevice));
+  ctx->rec_nz = n_z;
+  ctx->rec_nt = n_t;
+  ctx->rec_ng = n_gamma;
+  return RG_OK;
+}
+
 int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
                         rg_hii_scalars* out) {
   if (!ctx || !p || !s || !g || !out || !s->ZZ) return RG_EINVAL;
@@ -523,10 +589,14 @@ static int copy_grid(rg_context* ctx, void* dst, const void* src, size_t bytes, 
 static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
   const bool need_spin = p->Flag_IncludeSpinTemp != 0;
   const bool need_bh = p->Flag_BHFeedback != 0;
+  const bool need_rec = p->Flag_IncludeRecombinations != 0;
   if (ctx->dev_grids_ready) {
     const bool has_spin = ctx->dev_grids.Tk_box != nullptr;
     const bool has_bh = ctx->dev_grids.effective_bhm != nullptr;
-    if ((!need_spin || has_spin) && (!need_bh || has_bh) && ctx->dev_grids_nhist >= n_hist) return RG_OK;
+    const bool has_rec = ctx->dev_grids.Gamma12 != nullptr;
+    if ((!need_spin || has_spin) && (!need_bh || has_bh) && (!need_rec || has_rec) &&
+        ctx->dev_grids_nhist >= n_hist)
+      return RG_OK;
     for (void* q : ctx->owned) cudaFree(q);
     ctx->owned.clear();
     ctx->dev_grids_ready = false;
@@ -536,6 +606,37 @@ static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
   ctx->dev_grids_ready = true;
   ctx->dev_grids_nhist = n_hist;
   return RG_OK;
+}
+
+// Recombination branch of the host forms: N_rec, weighted_sfr and effective_bhar are then
+// transformed (they go with the first group of uploads); r_bubble and the recombination grids
+// come back after the step.
+static int hii_rec_inputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t cs) {
+  if (!p->Flag_IncludeRecombinations) return RG_OK;
+  const rg_grids& d = ctx->dev_grids;
+  const size_t n = (size_t)ctx->N;
+  const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float);
+  if (!h->N_rec || !h->Gamma12 || !h->residual_xH || !h->clumping_factor || !h->t_resp)
+    return set_error(ctx, RG_EINVAL, "recombinations need Gamma12, N_rec, residual_xH, clumping_factor, t_resp");
+  int rc = copy_grid(ctx, d.N_rec, h->N_rec, bp, cudaMemcpyHostToDevice, cs);
+  if (!rc && p->Flag_BHFeedback)
+    rc = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, cudaMemcpyHostToDevice, cs);
+  return rc;
+}
+
+static int hii_rec_outputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t st) {
+  if (!p->Flag_IncludeRecombinations) return RG_OK;
+  const rg_grids& d = ctx->dev_grids;
+  const size_t n = (size_t)ctx->N;
+  const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float), br = n * n * n * sizeof(float);
+  const auto D2H = cudaMemcpyDeviceToHost;
+  int rc;
+  if ((rc = copy_grid(ctx, h->r_bubble, d.r_bubble, br, D2H, st))) return rc;
+  if ((rc = copy_grid(ctx, h->Gamma12, d.Gamma12, br, D2H, st))) return rc;
+  if ((rc = copy_grid(ctx, h->N_rec, d.N_rec, bp, D2H, st))) return rc;
+  if ((rc = copy_grid(ctx, h->residual_xH, d.residual_xH, br, D2H, st))) return rc;
+  if ((rc = copy_grid(ctx, h->clumping_factor, d.clumping_factor, br, D2H, st))) return rc;
+  return copy_grid(ctx, h->t_resp, d.t_resp, br, D2H, st);
 }
 
 int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* h,
@@ -558,16 +659,21 @@ int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snaps
   if ((rc = copy_grid(ctx, (void*)d.deltax, h->deltax, bp, H2D, cs))) return rc;
   if ((rc = copy_grid(ctx, (void*)d.stars, h->stars, bp, H2D, cs))) return rc;
   if (p->Flag_IncludeSpinTemp && (rc = copy_grid(ctx, (void*)d.x_e_box, h->x_e_box, bp, H2D, cs))) return rc;
+  const bool rec = p->Flag_IncludeRecombinations != 0;
   if (p->Flag_BHFeedback && (rc = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D, cs))) return rc;
-  if (plain && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
+  if ((rc = hii_rec_inputs(ctx, p, h, cs))) return rc;
+  if ((plain || rec) && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
   if ((rc = stage_record(ctx, 1, cs, &stg.inputs))) return rc;
   if ((rc = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D, cs))) return rc;
   if ((rc = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D, cs))) return rc;
+  if (rec && (rc = copy_grid(ctx, d.Gamma12, h->Gamma12, br, H2D, cs))) return rc;
   if ((rc = stage_record(ctx, 2, cs, &stg.state))) return rc;
   if ((rc = copy_grid(ctx, d.temp_kinetic_all_gas, h->temp_kinetic_all_gas, br, H2D, cs))) return rc;
   if (p->Flag_IncludeSpinTemp && (rc = copy_grid(ctx, (void*)d.Tk_box, h->Tk_box, br, H2D, cs))) return rc;
-  if (!plain && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
-  if (p->Flag_BHFeedback && (rc = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D, cs))) return rc;
+  if (!plain && !rec && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
+  if (p->Flag_BHFeedback && !rec &&
+      (rc = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D, cs)))
+    return rc;
   if ((rc = stage_record(ctx, 3, cs, &stg.closing))) return rc;
   stg.host_r_bubble = h->r_bubble;
   rc = find_hii(ctx, p, s, &d, out, &stg);
@@ -580,6 +686,7 @@ int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snaps
   if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H))) return rc;
+  if ((rc = hii_rec_outputs(ctx, p, h, ctx->stream))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(cs));
   return RG_OK;
@@ -746,6 +853,7 @@ int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   const auto D2H = cudaMemcpyDeviceToHost;
   cudaStream_t cs = ctx->copy_stream, co = ctx->copy_stream_out, st = ctx->stream;
   const bool plain = ctx->mode == RG_MODE_PLAIN;
+  const bool rec = p->Flag_IncludeRecombinations != 0;
   auto fail = [&](int code) {
     cudaStreamSynchronize(cs);   // no copy of the caller's arrays outlives the call
     cudaStreamSynchronize(co);
@@ -761,15 +869,19 @@ int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   // find_HII's own grids: the state for its first z pass, the closing-pass grids
   auto hii_uploads = [&]() -> int {
     int r;
-    if (plain && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
+    if ((plain || rec) && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
     if (p->Flag_BHFeedback && (r = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D, cs))) return r;
+    if ((r = hii_rec_inputs(ctx, p, h, cs))) return r;
     if ((r = stage_record(ctx, 5, cs, &hs.inputs))) return r;
     if ((r = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D, cs))) return r;
     if ((r = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D, cs))) return r;
+    if (rec && (r = copy_grid(ctx, d.Gamma12, h->Gamma12, br, H2D, cs))) return r;
     if ((r = stage_record(ctx, 6, cs, &hs.state))) return r;
     if ((r = copy_grid(ctx, d.temp_kinetic_all_gas, h->temp_kinetic_all_gas, br, H2D, cs))) return r;
-    if (!plain && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
-    if (p->Flag_BHFeedback && (r = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D, cs))) return r;
+    if (!plain && !rec && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
+    if (p->Flag_BHFeedback && !rec &&
+        (r = copy_grid(ctx, (void*)d.effective_bhar, h->effective_bhar, bp, H2D, cs)))
+      return r;
     if (vel && (r = copy_grid(ctx, ctx->vel_stage, h->vel, bp, H2D, cs))) return r;   // delta_T, after find_HII
     return stage_record(ctx, 7, cs, &hs.closing);
   };
@@ -798,6 +910,7 @@ int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H, co))) return fail(rc);
   if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H, co))) return fail(rc);
   if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H, co))) return fail(rc);
+  if ((rc = hii_rec_outputs(ctx, p, h, co))) return fail(rc);
   if (h->delta_T) {
     rg_grids dd = d;
     if (vel) dd.vel = ctx->vel_stage;

@@ -178,8 +178,10 @@ __device__ __forceinline__ void block_sum(double (&acc)[K], double* out) {
 struct HiiBatch {
   int nr;             // radii in this batch
   int first;          // the batch starts the snapshot (state comes from z_at_ionization)
+  int ng;             // grids per radius (read by the instantiation for 5 to 7 grids)
   double fcoll_pref[KB_MAX];
   float J_aux[KB_MAX], J_aux_bh[KB_MAX];
+  float G_pref[KB_MAX], G_pref_bh[KB_MAX], R[KB_MAX];   // recombination branch
 };
 
 struct HiiState {
@@ -191,6 +193,8 @@ struct HiiState {
   const float* deltax_unf;   // padded
   const float* wsfr;         // padded
   const float* bhar;         // padded, may be null
+  float* Gamma12;            // recombination branch: written at a cell's first crossing
+  float* r_bubble;
   uint32_t* bits;            // [2][nblocks][W][NTH]
   double* partials;          // [nblocks][HII_NSUM]
 };
@@ -215,7 +219,9 @@ struct HiiZ {
 };
 
 // z pass of a batch.  FINAL: the batch ends with the snapshot's last (unfiltered) radius.
-// Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then effective_bhm (BH).
+// Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then effective_bhm (BH), then
+// with recombinations N_rec, weighted_sfr and effective_bhar (BH).  NG is the number of grids,
+// or 7 for any count from 5 to 7 (then bt.ng).
 template <int N, int NG, bool FINAL>
 __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
     k_hii_z(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
@@ -259,21 +265,25 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
       I[w] = s.bits[nwords + (blk * W + w) * NTH + threadIdx.x];
     }
   }
+  const int ng = NG == 7 ? bt.ng : NG;
   const int gx = c.spin ? 2 : -1;
   const int gb = c.bh ? (c.spin ? 3 : 2) : -1;
+  const int gn = c.rec ? 2 + c.spin + c.bh : -1;   // N_rec
+  const int gw = c.rec ? gn + 1 : -1;              // weighted_sfr
+  const int gr = c.rec && c.bh ? gn + 2 : -1;      // effective_bhar
   double acc[FINAL ? HII_NSUM : 1];
 #pragma unroll
   for (int k = 0; k < (FINAL ? HII_NSUM : 1); ++k) acc[k] = 0.0;
 
-  const int nunits = bt.nr * NG;   // (radius, grid) pairs, unit u = r * NG + g
+  const int nunits = bt.nr * ng;   // (radius, grid) pairs, unit u = r * ng + g
   ztile_issue<N, Q>(tiles, work, x, y0, NTH);
   cp_async_commit();
   const int q = threadIdx.x % Q, tq = threadIdx.x / Q;
   for (int r = 0; r < bt.nr; ++r) {
     __syncthreads();  // rt of the previous radius is consumed
 #pragma unroll 1
-    for (int g = 0; g < NG; ++g) {
-      const int u = r * NG + g;
+    for (int g = 0; g < ng; ++g) {
+      const int u = r * ng + g;
       cf* tile = tiles + (ZB == 2 ? (u & 1) : 0) * TB;
       if constexpr (ZB == 2) {
         if (u + 1 < nunits) ztile_issue<N, Q>(tiles + ((u + 1) & 1) * TB, work + (size_t)(u + 1) * stride, x, y0, NTH);
@@ -321,17 +331,41 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
           bhm = fmaxf(rt[(gb * ROWS + row) * RP + z], 0.f);
           if (bhm < ABS_TOL) bhm = 0.f;
         }
+        float nrec = 0.f;
+        if (gn >= 0) {
+          nrec = fmaxf(rt[(gn * ROWS + row) * RP + z], 0.f);
+          if (nrec < ABS_TOL) nrec = 0.f;
+        }
         const double dom = 1.0 + (double)dx;  // >= 1e-5 after the clamp
         const double nf = c.spin ? 1.0 - (double)xe : 1.0;
-        // (f_bh + f_stars) * prefactor > nf with f = grid / dom, tested without the division:
-        // the two forms differ only within a few FP64 ulps of the barrier
+        const double rec = gn >= 0 ? (double)nrec / dom : 0.0;
+        // (f_bh + f_stars) * prefactor > nf (1 + rec) with f = grid / dom, tested with both
+        // sides times dom: the two forms differ only within a few FP64 ulps of the barrier
         const double num = c.bh ? (double)bhm + (double)st : (double)st;
-        const bool ion = num * pref > nf * (1.0 + 0.0) * dom;
+        const bool ion = num * pref > nf * (1.0 + rec) * dom;
         float xH = (iw & bit) ? 0.f : 1.f;   // so far: 0 once ionized at a radius, else 1
         const size_t cellrow = (size_t)x * N + y0 + row;
         const size_t ir = cellrow * N + z;
         float temp_new = -1.f;               // >= 0: partial temperature written this radius
         if (ion) {
+          if (gn >= 0 && !(iw & bit)) {
+            // first crossing of the snapshot (find_HII_bubbles.c:488-508)
+            float wsf = fmaxf(rt[(gw * ROWS + row) * RP + z], 0.f);
+            if (wsf < ABS_TOL) wsf = 0.f;
+            float G = __fmul_rn(wsf, bt.G_pref[r]);
+            if (gr >= 0) {
+              float bhr = fmaxf(rt[(gr * ROWS + row) * RP + z], 0.f);
+              if (bhr < ABS_TOL) bhr = 0.f;
+              G = __fadd_rn(G, __fmul_rn(bhr, bt.G_pref_bh[r]));
+            }
+            s.Gamma12[ir] = G;
+            s.r_bubble[ir] = bt.R[r];
+            if (c.uvb == 2) {
+              float j = __fmul_rn(st, bt.J_aux[r]);
+              if (c.bh) j = __fadd_rn(j, __fmul_rn(bhm, bt.J_aux_bh[r]));
+              s.J21[ir] = j;
+            }
+          }
           xH = 0.f;
           iw |= bit;
         } else if (last && xH > REL_TOL) {
@@ -383,7 +417,7 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
           s.temp[ir] = temp;
           acc[0] += (double)xH;
           // acc[1] and acc[6]: r_bubble is written only on the recombination branch
-          // (find_HII_bubbles.c:490-508), which this library rejects, so it stays 0.
+          // (find_HII_bubbles.c:490-508); its sums come from k_hii_recomb.
           acc[2] += (double)s.wsfr[ip];
           if (s.bhar != nullptr) acc[3] += (double)s.bhar[ip];
           acc[4] += (double)temp;
@@ -427,6 +461,133 @@ __global__ void k_reduce_partials(const double* __restrict__ partials, int nbloc
 
 // ---------------------------------------------------------------------------
 // launchers
+
+// ---------------------------------------------------------------------------
+// recombinations in the closing pass (find_HII_bubbles.c:612-644)
+
+struct RecConst {
+  double redshift;     // ZZ[snapshot]
+  double hubble_h;
+  float fabs_dtdz;     // |dt/dz| / h at the snapshot, float as in the reference
+  float zstep;         // ZZ[snapshot - 1] - ZZ[snapshot] (0 at snapshot 0)
+  int temp_dep;        // Flag_TemperatureDependentRec
+};
+
+struct RecState {
+  const float* xH;
+  const float* temp;         // temp_kinetic_all_gas after the closing pass
+  const float* deltax_unf;   // padded
+  const float* r_bubble;
+  const float* Gamma12;
+  float* N_rec;              // padded
+  float* residual_xH;
+  float* clumping_factor;
+  float* t_resp;
+};
+
+constexpr int REC_NSUM = 10;   // r_bubble, Gamma12, N_rec, residual_xH, clumping: volume and mass
+constexpr int REC_NT = 256;
+
+// splined_recombination (recombinations.c:35-84): the (z, T) row by rounding to the nearest
+// sample, then the natural cubic spline in ln Gamma12 of that row.  The sample spacings are
+// the float constants of recombinations.h:17-34.
+__device__ void splined_recombination(const RecTables& t, double z_eff, double gamma12, double temp, double* rate,
+                                      double* rnh, double* cf) {
+  int z_ct = (int)((z_eff - (double)0.0f) / (double)0.2f + 0.5);
+  int t_ct = (int)((log10(temp) - (double)2.0f) / (double)0.03f + 0.5);
+  double lng = log(gamma12);
+  if (z_ct < 0)
+    z_ct = 0;
+  else if (z_ct >= t.nz)
+    z_ct = t.nz - 1;
+  if (t_ct < 0 || !(lng >= t.lng_lo)) {
+    *rate = 0.0;
+    *rnh = 1e4;
+    *cf = 1.0;
+    return;
+  }
+  if (t_ct >= t.nt) t_ct = t.nt - 1;
+  if (lng >= t.lng_hi) lng = t.lng_hi - 1e-7;   // FRACT_FLOAT_ERR
+  // interval lo with knots[lo] <= lng < knots[lo + 1]
+  int lo = 0, hi = t.ng - 1;
+  while (hi > lo + 1) {
+    const int mid = (lo + hi) >> 1;
+    if (t.knots[mid] > lng)
+      hi = mid;
+    else
+      lo = mid;
+  }
+  const double xlo = t.knots[lo];
+  const double h = t.knots[lo + 1] - xlo, dx = lng - xlo;
+  const size_t rows = (size_t)t.nz * t.nt;
+  const size_t row = (size_t)z_ct * t.nt + t_ct;
+  double v[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const size_t o = ((size_t)k * rows + row) * t.ng + lo;
+    const double yl = t.y[o], yh = t.y[o + 1], cl = t.c[o], ch = t.c[o + 1];
+    const double b = (yh - yl) / h - h * (ch + 2.0 * cl) / 3.0;
+    const double d = (ch - cl) / (3.0 * h);
+    v[k] = yl + dx * (b + dx * (cl + dx * d));
+  }
+  *rate = exp(v[0]);
+  *cf = v[1];
+  *rnh = exp(v[2]);
+}
+
+template <int N>
+__global__ void __launch_bounds__(REC_NT) k_hii_recomb(RecTables tab, RecConst c, RecState s, double* partials) {
+  constexpr int PADW = 2 * (N / 2 + 1);
+  const size_t n3 = (size_t)N * N * N;
+  double acc[REC_NSUM];
+#pragma unroll
+  for (int k = 0; k < REC_NSUM; ++k) acc[k] = 0.0;
+  for (size_t ir = (size_t)blockIdx.x * REC_NT + threadIdx.x; ir < n3; ir += (size_t)gridDim.x * REC_NT) {
+    const size_t ip = ir / N * PADW + ir % N;
+    const float xHf = s.xH[ir];
+    const double dom = 1.0 + (double)s.deltax_unf[ip];
+    const double z_eff = (1.0 + c.redshift) * pow(dom, 1.0 / 3.0) - 1.0;
+    const double temp = c.temp_dep ? (double)s.temp[ir] : 1e4;
+    const float G = s.Gamma12[ir];
+    const double gh = __dmul_rn(__dmul_rn((double)G, c.hubble_h), c.hubble_h);
+    double rate, rnh, cf;
+    splined_recombination(tab, z_eff, gh, temp, &rate, &rnh, &cf);
+    // N_rec += (float)rate * fabs_dtdz * zstep * (1 - xH): a float product, widened
+    const float f = __fmul_rn(__fmul_rn((float)rate, c.fabs_dtdz), c.zstep);
+    const float nrec = (float)__dadd_rn((double)s.N_rec[ip], __dmul_rn((double)f, 1.0 - (double)xHf));
+    s.N_rec[ip] = nrec;
+    const float rnhf = (float)rnh, cff = (float)cf;
+    s.residual_xH[ir] = rnhf;
+    s.clumping_factor[ir] = cff;
+    // t_resp = 1 / (Gamma + rate) in Myr, stored as float first (find_HII_bubbles.c:630-635)
+    float tr = (float)__dadd_rn(__dmul_rn(gh, 1e-12), rate);
+    tr = tr > 0.f ? (float)(1.0 / (double)tr / SEC_PER_MEGAYEAR) : 1e30f;
+    s.t_resp[ir] = tr;
+    const double rb = (double)s.r_bubble[ir];
+    acc[0] += rb;
+    acc[1] += rb * dom;
+    acc[2] += (double)G;
+    acc[3] += (double)G * dom;
+    acc[4] += (double)nrec;
+    acc[5] += (double)nrec * dom;
+    acc[6] += (double)rnhf;
+    acc[7] += (double)rnhf * dom;
+    acc[8] += (double)cff;
+    acc[9] += (double)cff * dom;
+  }
+  block_sum<REC_NT, REC_NSUM>(acc, partials + (size_t)blockIdx.x * REC_NSUM);
+}
+
+template <int N>
+int launch_hii_recomb(rg_context* ctx, const RecTables& tab, const RecConst& c, const RecState& s, double* partials,
+                      int nblocks, cudaStream_t st) {
+  prof_begin(ctx, "hii_recomb", st);
+  k_hii_recomb<N><<<nblocks, REC_NT, 0, st>>>(tab, c, s, partials);
+  // xH, temperature, deltax, r_bubble, Gamma12 read; N_rec read and written; three outputs
+  prof_end(ctx, 40.0 * (double)N * N * N, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  return RG_OK;
+}
 
 template <typename K>
 static cudaError_t prep(K kernel, size_t smem) {
@@ -523,6 +684,7 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using C = Cfg<N>;
+  static_assert(HiiZ<N, FINAL>::smem(NG) <= 227 * 1024, "z pass shared memory above the per-block limit");
   const size_t sm = HiiZ<N, FINAL>::smem(NG);
   RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL>, sm));
   const dim3 grid(N / (2 * C::QZ), N);
@@ -530,7 +692,7 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   // first batch; the closing pass writes xH and temperature and reads deltax, weighted_sfr,
   // [effective_bhar], [Tk_box]
   const double n3 = (double)N * N * N, nzc = (double)C::NZ * N * N;
-  double bytes = bt.nr * NG * 8.0 * nzc + (bt.first ? 4.0 * n3 : 0.0);
+  double bytes = bt.nr * (NG == 7 ? bt.ng : NG) * 8.0 * nzc + (bt.first ? 4.0 * n3 : 0.0);
   if (FINAL) bytes += 4.0 * n3 * (2 + 2 + (s.bhar != nullptr) + (s.Tk_box != nullptr));
   prof_begin(ctx, FINAL ? "inv_z_c2r_test_final" : "inv_z_c2r_test", st);
   k_hii_z<N, NG, FINAL><<<grid, C::T * C::QZ, sm, st>>>(work, stride, tw, bt, c, s);
@@ -549,8 +711,12 @@ int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const H
   if (ng == 3)
     return fin ? launch_hii_z3<N, 3, true>(ctx, work, stride, bt, c, s, st, nblocks)
                : launch_hii_z3<N, 3, false>(ctx, work, stride, bt, c, s, st, nblocks);
-  return fin ? launch_hii_z3<N, 4, true>(ctx, work, stride, bt, c, s, st, nblocks)
-             : launch_hii_z3<N, 4, false>(ctx, work, stride, bt, c, s, st, nblocks);
+  if (ng == 4)
+    return fin ? launch_hii_z3<N, 4, true>(ctx, work, stride, bt, c, s, st, nblocks)
+               : launch_hii_z3<N, 4, false>(ctx, work, stride, bt, c, s, st, nblocks);
+  // 5 to 7 grids (recombinations): one instantiation reads the count from the batch
+  return fin ? launch_hii_z3<N, 7, true>(ctx, work, stride, bt, c, s, st, nblocks)
+             : launch_hii_z3<N, 7, false>(ctx, work, stride, bt, c, s, st, nblocks);
 }
 
 // words of packed state per bit kind
@@ -630,6 +796,11 @@ static int hii_z(rg_context* ctx, int n, const cf* work, size_t stride, int ng, 
 
 static size_t bit_words(int n) { RG_DISPATCH_N_VAL(n, hii_bit_words<NN>(), (size_t)0); }
 
+static int hii_recomb(rg_context* ctx, int n, const RecTables& tab, const RecConst& c, const RecState& s,
+                      double* partials, int nblocks, cudaStream_t st) {
+  RG_DISPATCH_N(n, launch_hii_recomb<NN>(ctx, tab, c, s, partials, nblocks, st));
+}
+
 int window_table(rg_context* ctx, double box, const double* d_radii, int nr, int ftype, float* d_wtab, int n2max,
                  cudaStream_t st, int* d_wcut) {
   const double delta_k = 2.0 * M_PI / box;
@@ -677,6 +848,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   cudaStream_t st = ctx->stream;
   const int N = ctx->N;
   const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
+  const bool rec = p->Flag_IncludeRecombinations != 0;
   const double redshift = s->ZZ[s->snapshot];
   const double box_size = p->BoxSize;
   const double pixel_volume = std::pow(box_size / (double)N, 3);
@@ -691,19 +863,26 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   c.uvb = p->ReionUVBFlag;
   c.spin = spin;
   c.bh = bh;
+  c.rec = rec;
 
-  // Grids to transform: the ones the barrier test reads, in its order.  weighted_sfr (and
-  // effective_bhar) feed only Gamma12 on the recombination branch, so their filtered fields
-  // are never read here; the plain mode transforms weighted_sfr anyway, as the reference does.
-  const float* srcs[5];
+  // Grids to transform: the ones the z pass reads, in its order.  weighted_sfr (and
+  // effective_bhar) feed only Gamma12 on the recombination branch, so without it their
+  // filtered fields are never read; the plain mode transforms weighted_sfr anyway, as the
+  // reference does.
+  const float* srcs[8];
   int ng = 0;
   srcs[ng++] = g->deltax;
   srcs[ng++] = g->stars;
   if (spin) srcs[ng++] = g->x_e_box;
   if (bh) srcs[ng++] = g->effective_bhm;
+  if (rec) {
+    srcs[ng++] = g->N_rec;
+    srcs[ng++] = g->weighted_sfr;
+    if (bh) srcs[ng++] = g->effective_bhar;
+  }
   const int ntest = ng;
   const bool plain = ctx->mode == RG_MODE_PLAIN;
-  if (plain) srcs[ng++] = g->weighted_sfr;
+  if (plain && !rec) srcs[ng++] = g->weighted_sfr;
 
   const size_t nc = (size_t)(N / 2 + 1) * N * N;
   auto sched = radius_schedule(p, redshift);
@@ -732,7 +911,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
 
   // r_bubble is only written on the recombination branch: zero it once
   RG_CUDA_TRY(ctx, cudaMemsetAsync(g->r_bubble, 0, sizeof(float) * (size_t)N * N * N, st));
-  if (stg->host_r_bubble) {
+  if (stg->host_r_bubble && !rec) {
     // final already: the host copy overlaps the radius loop
     cudaEvent_t e;
     if ((rc = stage_record(ctx, 4, st, &e))) return rc;
@@ -740,7 +919,8 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(stg->host_r_bubble, g->r_bubble, sizeof(float) * (size_t)N * N * N,
                                      cudaMemcpyDeviceToHost, ctx->copy_stream));
   }
-  double* partials = ensure_partials(ctx, (size_t)N * N * HII_NSUM);
+  double* partials =
+      ensure_partials(ctx, std::max((size_t)N * N * HII_NSUM, (size_t)4 * ctx->num_sms * REC_NSUM));
   if (!partials) return set_error(ctx, RG_ENOMEM, "partials");
 
   HiiState hs;
@@ -752,6 +932,8 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   hs.deltax_unf = g->deltax;
   hs.wsfr = g->weighted_sfr;
   hs.bhar = bh ? g->effective_bhar : nullptr;
+  hs.Gamma12 = g->Gamma12;
+  hs.r_bubble = g->r_bubble;
   hs.bits = ctx->bits;
   hs.partials = partials;
 
@@ -764,6 +946,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     std::memset(&bt, 0, sizeof(bt));
     bt.nr = cnt;
     bt.first = (r0 == 0);
+    bt.ng = ntest;
     for (int k = 0; k < cnt; ++k) {
       const double R = sched[r0 + k].first;
       const double M_mean = rtom(p, R);
@@ -775,6 +958,11 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
                             p->ReionAlphaUV);
       bt.J_aux_bh[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias /
                                sfr_timescale * p->ReionAlphaUVBH);
+      const double G_bh = Gamma_R_prefactor * (SIGMA_HI * p->ReionAlphaUVBH / (p->ReionAlphaUVBH + 2.75) * 1e12);
+      Gamma_R_prefactor *= SIGMA_HI * p->ReionAlphaUV / (p->ReionAlphaUV + 2.75) * 1e12;
+      bt.G_pref[k] = (float)Gamma_R_prefactor;
+      bt.G_pref_bh[k] = (float)G_bh;
+      bt.R[k] = (float)R;
       bt.fcoll_pref[k] = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R * R * R;
     }
     // the snapshot's last radius is unfiltered (find_HII_bubbles.c:313)
@@ -787,7 +975,39 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     if ((rc = hii_z(ctx, N, ctx->work, nc, ntest, bt, c, hs, fin, st, &nblocks))) return rc;
   }
   if ((rc = reduce_partials(ctx, partials, nblocks, HII_NSUM, ctx->d_sums, st))) return rc;
-  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * HII_NSUM, cudaMemcpyDeviceToHost, st));
+  if (rec) {
+    RecTables tab;
+    tab.knots = ctx->rec_knots;
+    tab.y = ctx->rec_y;
+    tab.c = ctx->rec_c;
+    tab.nz = ctx->rec_nz;
+    tab.nt = ctx->rec_nt;
+    tab.ng = ctx->rec_ng;
+    // recombinations.c:51-64: the table's bounds as the float expressions of the C
+    tab.lng_lo = (double)(-10.0f);
+    tab.lng_hi = (double)(-10.0f + 0.1f * (float)(ctx->rec_ng - 1));
+    RecConst rcst;
+    rcst.redshift = redshift;
+    rcst.hubble_h = p->Hubble_h;
+    const double prev_z = s->snapshot == 0 ? redshift : s->ZZ[s->snapshot - 1];
+    rcst.zstep = (float)(prev_z - redshift);
+    rcst.fabs_dtdz = (float)std::fabs(dtdz(p, (float)redshift) / p->Hubble_h);
+    rcst.temp_dep = p->Flag_TemperatureDependentRec != 0;
+    RecState rs;
+    rs.xH = g->xH;
+    rs.temp = g->temp_kinetic_all_gas;
+    rs.deltax_unf = g->deltax;
+    rs.r_bubble = g->r_bubble;
+    rs.Gamma12 = g->Gamma12;
+    rs.N_rec = g->N_rec;
+    rs.residual_xH = g->residual_xH;
+    rs.clumping_factor = g->clumping_factor;
+    rs.t_resp = g->t_resp;
+    const int rb = 4 * ctx->num_sms;
+    if ((rc = hii_recomb(ctx, N, tab, rcst, rs, partials, rb, st))) return rc;
+    if ((rc = reduce_partials(ctx, partials, rb, REC_NSUM, ctx->d_sums + 16, st))) return rc;
+  }
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_sums, ctx->d_sums, sizeof(double) * 32, cudaMemcpyDeviceToHost, st));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   prof_resolve(ctx);
   if ((rc = xy_ctrl_check(ctx, st))) return rc;
@@ -805,6 +1025,19 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   out->mass_weighted_global_r_bubble = S[6] / mass_weight;
   out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
   out->n_radii = nr;
+  const double* R = S + 16;   // recombination sums (find_HII_bubbles.c:666-684)
+  out->volume_weighted_global_Gamma12 = rec ? R[2] / n3 : 0.0;
+  out->volume_weighted_global_N_rec = rec ? R[4] / n3 : 0.0;
+  out->volume_weighted_global_residual_xH = rec ? R[6] / n3 : 0.0;
+  out->volume_weighted_global_clumping_factor = rec ? R[8] / n3 : 0.0;
+  out->mass_weighted_global_Gamma12 = rec ? R[3] / mass_weight : 0.0;
+  out->mass_weighted_global_N_rec = rec ? R[5] / mass_weight : 0.0;
+  out->mass_weighted_global_residual_xH = rec ? R[7] / mass_weight : 0.0;
+  out->mass_weighted_global_clumping_factor = rec ? R[9] / mass_weight : 0.0;
+  if (rec) {
+    out->volume_weighted_global_r_bubble = R[0] / n3;
+    out->mass_weighted_global_r_bubble = R[1] / mass_weight;
+  }
   return RG_OK;
 }
 

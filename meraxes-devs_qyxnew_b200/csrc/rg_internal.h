@@ -93,7 +93,16 @@ int ensure_device(rg_context* ctx, T** ptr, size_t* have, size_t need) {
 // Per-snapshot constants of the barrier test.
 struct HiiConst {
   float redshift, TK, cT_ad;
-  int uvb, spin, bh;
+  int uvb, spin, bh, rec;
+};
+
+// Recombination tables on the device (splined_recombination, recombinations.c:35-84).
+struct RecTables {
+  const double* knots;   // ln Gamma12 knots [ng]
+  const double* y;       // [3][nz * nt][ng]: ln RR, CF, ln RNH
+  const double* c;       // natural-spline coefficients, same layout
+  int nz, nt, ng;
+  double lng_lo, lng_hi; // knots[0] and the float-rounded upper bound of the table
 };
 
 constexpr int HII_NSUM = 9;   // closing-pass sums
@@ -191,6 +200,12 @@ struct rg_context {
   size_t vel_stage_elems = 0;
   int* ngp_bad = nullptr;        // rg_deposit_ngp: count of galaxies below the box
   size_t ngp_bad_elems = 0;
+  // recombination tables (rg_set_recombination_tables): knots, and per table and (z, T) row the
+  // values and the natural-spline coefficients c (half the second derivative), [3][nz*nt][ng]
+  double* rec_knots = nullptr;
+  double* rec_y = nullptr;
+  double* rec_c = nullptr;
+  int rec_nz = 0, rec_nt = 0, rec_ng = 0;
   double* partials = nullptr;
   size_t partials_elems = 0;
   double* d_sums = nullptr;      // reduced sums

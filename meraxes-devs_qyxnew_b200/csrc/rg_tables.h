@@ -17,6 +17,7 @@ class CubicSpline {
   double eval(double x) const;        // caller keeps x inside [x0, x_{n-1}]
   size_t size() const { return x_.size(); }
   const std::vector<double>& xs() const { return x_; }
+  const std::vector<double>& half_curvature() const { return c_; }   // c_i = y''_i / 2
   // per interval i: y = a + dx (b + dx (c + dx d)), dx = x - x_i
   void coeffs(size_t i, double* a, double* b, double* c, double* d) const;
 

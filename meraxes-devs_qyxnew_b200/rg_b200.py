@@ -41,6 +41,7 @@ class rg_params(C.Structure):
         ("Flag_IncludePecVelsFor21cm", C.c_int),
         ("TablesForXHeatingDir", C.c_char_p),
         ("TreesID", C.c_int),
+        ("Flag_TemperatureDependentRec", C.c_int),
     ]
 
 
@@ -59,6 +60,8 @@ class rg_grids(C.Structure):
         ("n_hist", C.c_int),
         ("delta_T", C.c_void_p),
         ("vel", C.c_void_p),
+        ("Gamma12", C.c_void_p), ("N_rec", C.c_void_p), ("residual_xH", C.c_void_p),
+        ("clumping_factor", C.c_void_p), ("t_resp", C.c_void_p),
     ]
 
 
@@ -72,7 +75,10 @@ class rg_hii_scalars(C.Structure):
         "volume_weighted_global_xH", "volume_weighted_global_r_bubble", "volume_weighted_global_weighted_sfr",
         "volume_weighted_global_effective_bhar", "volume_weighted_global_temp_kinetic_all_gas",
         "mass_weighted_global_xH", "mass_weighted_global_r_bubble", "mass_weighted_global_temp_kinetic_all_gas")] + [
-        ("n_radii", C.c_int)]
+        ("n_radii", C.c_int)] + [(n, C.c_double) for n in (
+        "volume_weighted_global_Gamma12", "volume_weighted_global_N_rec", "volume_weighted_global_residual_xH",
+        "volume_weighted_global_clumping_factor", "mass_weighted_global_Gamma12", "mass_weighted_global_N_rec",
+        "mass_weighted_global_residual_xH", "mass_weighted_global_clumping_factor")]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -123,6 +129,8 @@ _SIGS = {
     "rg_power_spectrum_host": (C.c_int, [C.c_void_p, _P(rg_params), C.c_void_p, C.c_int, _P(C.c_float),
                                          _P(C.c_float), _P(C.c_float), _P(C.c_int)]),
     "rg_smooth_grid": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p]),
+    "rg_set_recombination_tables": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                              C.c_void_p, C.c_void_p]),
     "rg_deposit_ngp": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                  C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
     "rg_radius_schedule": (C.c_int, [_P(rg_params), C.c_double, _P(C.c_double), C.c_int, _P(C.c_int)]),
@@ -258,6 +266,14 @@ class Context:
         m = n.value
         return (np.frombuffer(k, np.float32)[:m].copy(), np.frombuffer(d, np.float32)[:m].copy(),
                 np.frombuffer(e, np.float32)[:m].copy())
+
+    def set_recombination_tables(self, lnGamma, RR, CF, RNH):
+        """The MHR tables (RR and RNH as natural logs), each [nz][nt][ng] float64."""
+        import numpy as np
+        k = np.ascontiguousarray(lnGamma, np.float64)
+        tabs = [np.ascontiguousarray(a, np.float64) for a in (RR, CF, RNH)]
+        nz, nt, ng = tabs[0].shape
+        self.call("rg_set_recombination_tables", k.ctypes.data, nz, nt, ng, *(a.ctypes.data for a in tabs))
 
     def deposit_ngp(self, box_size: float, n_gal: int, pos_ptr: int, values_ptr: int, grid_ptrs, divisors=None):
         """Nearest-grid-point deposit of n_gal galaxies (device positions [n_gal][3] and values

@@ -94,6 +94,7 @@ class Params:
     NuXraySoftCut: float = 2000.0
     NuXrayMax: float = 10000.0
     SpecIndexXrayGal: float = 1.0
+    Flag_TemperatureDependentRec: int = 1
 
 
 @dataclasses.dataclass
@@ -282,16 +283,23 @@ class HIIState:
     z_at_ionization: np.ndarray            # [N^3] float32, -1 = never
     J_21_at_ionization: np.ndarray         # [N^3] float32
     temp_kinetic_all_gas: np.ndarray       # [N^3] float32
+    Gamma12: np.ndarray | None = None      # recombinations: [N^3] float32
+    N_rec: np.ndarray | None = None        # recombinations: [N^3] float32 (real part of the padded grid)
 
     @staticmethod
-    def fresh(n: int) -> "HIIState":
-        """init_reion_grids() values (src/core/reionization.c:557-595)."""
-        return HIIState(np.full((n, n, n), -1.0, np.float32), np.zeros((n, n, n), np.float32),
-                        np.zeros((n, n, n), np.float32))
+    def fresh(n: int, rec: bool = False) -> "HIIState":
+        """init_reion_grids() values (src/core/reionization.c:557-595,698)."""
+        st = HIIState(np.full((n, n, n), -1.0, np.float32), np.zeros((n, n, n), np.float32),
+                      np.zeros((n, n, n), np.float32))
+        if rec:
+            st.Gamma12 = np.zeros((n, n, n), np.float32)
+            st.N_rec = np.zeros((n, n, n), np.float32)
+        return st
 
     def copy(self) -> "HIIState":
+        c = lambda a: None if a is None else a.copy()
         return HIIState(self.z_at_ionization.copy(), self.J_21_at_ionization.copy(),
-                        self.temp_kinetic_all_gas.copy())
+                        self.temp_kinetic_all_gas.copy(), c(self.Gamma12), c(self.N_rec))
 
 
 def hii_scalars_names() -> list[str]:
@@ -305,8 +313,16 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
                      state: HIIState, precision: str = "fp32", x_e_box: np.ndarray | None = None,
                      Tk_box: np.ndarray | None = None, effective_bhm: np.ndarray | None = None,
                      effective_bhar: np.ndarray | None = None, record_margins: bool = False,
-                     radius_subset: int | None = None, with_dead_grids: bool = False):
-    """Restatement of _find_HII_bubbles() (find_HII_bubbles.c:86-710), one rank, no recombinations.
+                     radius_subset: int | None = None, with_dead_grids: bool = False, rec_tables=None,
+                     prev_z: float | None = None):
+    """Restatement of _find_HII_bubbles() (find_HII_bubbles.c:86-710), one rank.
+
+    With ``Flag_IncludeRecombinations`` the state carries Gamma12 and N_rec, ``rec_tables`` is a
+    ``rec_oracle.RecTables`` and ``prev_z`` the previous snapshot's redshift (``z`` at the first
+    snapshot); N_rec and weighted_sfr (and effective_bhar) are filtered too, the barrier is
+    tested against 1 + N_rec (:467-483), Gamma12, r_bubble (and J_21 for ReionUVBFlag 2) are
+    recorded at each cell's first crossing (:488-508), and the closing pass updates N_rec and
+    returns residual_xH, clumping_factor and t_resp in ``diag["rec"]`` (:612-644).
 
     Inputs are padded float32 grids; ``state`` is updated in place.  Returns
     ``(xH, r_bubble, scalars, diag)`` where ``diag`` holds, when
@@ -320,8 +336,9 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     """
     import time as _time
     t_start = _time.perf_counter()
-    if p.Flag_IncludeRecombinations:
-        raise NotImplementedError("recombinations are not restated")
+    rec = bool(p.Flag_IncludeRecombinations)
+    if rec and (rec_tables is None or state.Gamma12 is None or state.N_rec is None):
+        raise ValueError("recombinations need rec_tables and a state with Gamma12 and N_rec")
     n = p.ReionGridDim
     box = p.BoxSize
     u = run_units(p)
@@ -343,6 +360,11 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
         grids["x_e"] = x_e_box[:, :, :n]
     if p.Flag_BHFeedback:
         grids["bhm"] = effective_bhm[:, :, :n]
+    if rec:
+        grids["nrec"] = state.N_rec
+        grids["wsfr"] = weighted_sfr[:, :, :n]
+        if p.Flag_BHFeedback:
+            grids["bhar"] = effective_bhar[:, :, :n]
     if with_dead_grids:
         grids["wsfr"] = weighted_sfr[:, :, :n]
     spectra = {k: forward(v, precision) for k, v in grids.items()}
@@ -390,19 +412,40 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
             fb = np.maximum(fb, 0).astype(fb.dtype)
             fb = np.where(fb < (ABS_TOL if precision == "fp32" else float(ABS_TOL)), 0, fb).astype(fb.dtype)
 
+        def clamped(key):
+            f = filt[key]
+            f = np.maximum(f, 0).astype(f.dtype)
+            return np.where(f < (ABS_TOL if precision == "fp32" else float(ABS_TOL)), 0, f).astype(f.dtype)
+
         M_mean = rtom(p, R)
         g_pref = ((1.0 + z) * (1.0 + z) * R * p.UnitLength_in_cm / pixel_volume * p.UnitLength_in_cm ** -3.0)
         g_pref *= (p.UnitMass_in_g / u.UnitTime_in_s) / PROTONMASS * p.ReionNionPhotPerBary
         J_aux = f32(g_pref * PLANCK * 1e21 / (4.0 * math.pi) * p.ReionGammaHaloBias / sfr_timescale * p.ReionAlphaUV)
         J_aux_bh = f32(g_pref * PLANCK * 1e21 / (4.0 * math.pi) * p.ReionGammaHaloBias / sfr_timescale * p.ReionAlphaUVBH)
         fcoll_pref = p.ReionEfficiency * (4.0 / 3.0) * math.pi / pixel_volume / M_mean * R ** 3
+        G_pref_bh = g_pref * (SIGMA_HI * p.ReionAlphaUVBH / (p.ReionAlphaUVBH + 2.75) * 1e12)
+        G_pref = g_pref * (SIGMA_HI * p.ReionAlphaUV / (p.ReionAlphaUV + 2.75) * 1e12)
 
         dom = 1.0 + fd.astype(np.float64)
         fcs = fs.astype(np.float64) / dom
         fbh = fb.astype(np.float64) / dom if fb is not None else 0.0
         lhs = (fbh + fcs) * fcoll_pref
-        rhs = neutral * (1.0 + 0.0)
+        recf = clamped("nrec").astype(np.float64) / dom if rec else 0.0
+        rhs = neutral * (1.0 + recf)
         ion = lhs > rhs
+        if rec:
+            # first crossing of the snapshot (find_HII_bubbles.c:488-508)
+            first = ion & (xH > REL_TOL)
+            gam = (clamped("wsfr")[first].astype(f32) * f32(G_pref)).astype(f32)
+            if p.Flag_BHFeedback:
+                gam = (gam + (clamped("bhar")[first].astype(f32) * f32(G_pref_bh)).astype(f32)).astype(f32)
+            state.Gamma12[first] = gam
+            r_bubble[first] = f32(R)
+            if p.ReionUVBFlag == 2:
+                jj = (fs[first].astype(f32) * J_aux).astype(f32)
+                if fb is not None:
+                    jj = (jj + (fb[first].astype(f32) * J_aux_bh).astype(f32)).astype(f32)
+                J21[first] = jj
         if record_margins:
             m = np.abs(lhs / rhs - 1.0)
             np.minimum(min_margin, m, out=min_margin)
@@ -456,8 +499,33 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     s["mass_weighted_global_xH"] = (xH.astype(np.float64) * dom).sum() / mw
     s["mass_weighted_global_r_bubble"] = (r_bubble.astype(np.float64) * dom).sum() / mw
     s["mass_weighted_global_temp_kinetic_all_gas"] = (temp.astype(np.float64) * dom).sum() / mw
+    rec_out = None
+    if rec:
+        # closing pass with recombinations (find_HII_bubbles.c:612-644)
+        h = p.Hubble_h
+        z_eff = (1.0 + z) * dom ** (1.0 / 3.0) - 1.0
+        trec = temp.astype(np.float64) if p.Flag_TemperatureDependentRec else np.full(dom.shape, 1e4)
+        gam = state.Gamma12.astype(np.float64) * h * h
+        rate, rnh, cf = rec_tables.splined(z_eff, gam, trec)
+        zstep = f32((z if prev_z is None else prev_z) - z)
+        fabs_dtdz = f32(abs(dtdz(p, float(f32(z))) / h))
+        inc = ((rate.astype(f32) * fabs_dtdz).astype(f32) * zstep).astype(f32)
+        state.N_rec[:] = (state.N_rec.astype(np.float64) + inc.astype(np.float64) *
+                          (1.0 - xH.astype(np.float64))).astype(f32)
+        residual = rnh.astype(f32)
+        clump = cf.astype(f32)
+        tr = (gam * 1e-12 + rate).astype(f32)
+        with np.errstate(divide="ignore"):
+            t_resp = np.where(tr > 0, (1.0 / tr.astype(np.float64) / SEC_PER_MEGAYEAR).astype(f32), f32(1e30))
+        rec_out = {"residual_xH": residual, "clumping_factor": clump, "t_resp": t_resp.astype(f32)}
+        for name, a in (("Gamma12", state.Gamma12), ("N_rec", state.N_rec), ("residual_xH", residual),
+                        ("clumping_factor", clump)):
+            s["volume_weighted_global_" + name] = a.astype(np.float64).sum() / n3
+            s["mass_weighted_global_" + name] = (a.astype(np.float64) * dom).sum() / mw
+        s["volume_weighted_global_r_bubble"] = r_bubble.astype(np.float64).sum() / n3
+        s["mass_weighted_global_r_bubble"] = (r_bubble.astype(np.float64) * dom).sum() / mw
     t_final = _time.perf_counter() - t_f0
-    diag = {"min_margin": min_margin, "first_cross": first_cross, "n_radii": len(sched),
+    diag = {"min_margin": min_margin, "first_cross": first_cross, "n_radii": len(sched), "rec": rec_out,
             "timing": {"forward": t_forward, "per_radius": float(np.mean(radius_times)), "final": t_final}}
     return xH, r_bubble, s, diag
 

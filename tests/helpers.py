@@ -34,7 +34,7 @@ def install_recfast():
 class DeviceGrids:
     """torch CUDA buffers for an rg_grids struct."""
 
-    def __init__(self, n: int, spin: bool = False, bh: bool = False):
+    def __init__(self, n: int, spin: bool = False, bh: bool = False, rec: bool = False):
         import torch
         self.torch = torch
         self.n = n
@@ -52,6 +52,9 @@ class DeviceGrids:
                            "sfr": z(npad), "xray_luminosity": z(npad)})
         if bh:
             self.t.update({"effective_bhm": z(npad), "effective_bhar": z(npad)})
+        if rec:
+            self.t.update({"Gamma12": z(nreal), "N_rec": z(npad), "residual_xH": z(nreal),
+                           "clumping_factor": z(nreal), "t_resp": torch.full((nreal,), 1e30, device=dev)})
         self.g = rg.rg_grids()
         for k, v in self.t.items():
             setattr(self.g, k, v.data_ptr())

@@ -7,6 +7,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import rec_oracle as rco
 import rg_b200 as rg
 import workloads as wl
 from helpers import DeviceGrids
@@ -43,7 +44,16 @@ def test_find_hii_rejections_leave_context_usable():
     base = dict(Flag_EvolvingReionRBubbleMax=0, ReionRBubbleMax=20.0, ReionEfficiency=2000.0)
     assert run(rg.make_params(32, 20.0, **base)) == rg.RG_EINVAL                       # N differs
     assert "ReionGridDim" in ctx.lib.rg_last_error(ctx.h).decode()
-    assert run(rg.make_params(n, 20.0, Flag_IncludeRecombinations=1, **base)) == rg.RG_EUNSUPPORTED
+    # recombinations: the tables first, then the recombination grids
+    assert run(rg.make_params(n, 20.0, Flag_IncludeRecombinations=1, **base)) == rg.RG_EINVAL
+    assert "rg_set_recombination_tables" in ctx.lib.rg_last_error(ctx.h).decode()
+    t = rco.synthetic_tables(8, 6, 150)
+    ctx.set_recombination_tables(t.knots, *(t.y[k].reshape(8, 6, 150) for k in range(3)))
+    assert run(rg.make_params(n, 20.0, Flag_IncludeRecombinations=1, **base)) == rg.RG_EINVAL   # no N_rec
+    bad_knots = t.knots.copy()
+    bad_knots[5] = bad_knots[4]
+    with pytest.raises(rg.RGError):
+        ctx.set_recombination_tables(bad_knots, *(t.y[k].reshape(8, 6, 150) for k in range(3)))
     assert run(rg.make_params(n, 20.0, ReionFilterType=3, **base)) == rg.RG_EINVAL
     assert run(rg.make_params(n, 20.0, ReionDeltaRFactor=1.0, **base)) == rg.RG_EINVAL
     assert run(rg.make_params(n, 20.0, **base), s=rg.snapshot(zz, len(zz) + 3)) == rg.RG_EINVAL

@@ -272,7 +272,7 @@ def test_invalid_parameters_rejected():
     s = rg.snapshot(zz, snap)
     out = rg.rg_hii_scalars()
     lib = rg.load()
-    for kw, status in [({"ReionFilterType": 3}, rg.RG_EINVAL), ({"Flag_IncludeRecombinations": 1}, rg.RG_EUNSUPPORTED),
+    for kw, status in [({"ReionFilterType": 3}, rg.RG_EINVAL), ({"Flag_IncludeRecombinations": 1}, rg.RG_EINVAL),
                        ({"ReionGridDim": 32}, rg.RG_EINVAL), ({"ReionDeltaRFactor": 0.9}, rg.RG_EINVAL)]:
         p = rg.make_params(n, 16.0, **kw)
         assert lib.rg_find_HII_bubbles(ctx.h, C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out)) == status, kw
