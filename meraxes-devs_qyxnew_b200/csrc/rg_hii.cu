@@ -221,7 +221,7 @@ struct HiiZ {
 // z pass of a batch.  FINAL: the batch ends with the snapshot's last (unfiltered) radius.
 // Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then effective_bhm (BH), then
 // with recombinations N_rec, weighted_sfr and effective_bhar (BH).  NG is the number of grids,
-// or 7 for any count from 5 to 7 (then bt.ng).
+// or 7 for any count from 4 to 7 (then bt.ng), which is the one used with recombinations.
 template <int N, int NG, bool FINAL>
 __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
     k_hii_z(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
@@ -268,9 +268,12 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
   const int ng = NG == 7 ? bt.ng : NG;
   const int gx = c.spin ? 2 : -1;
   const int gb = c.bh ? (c.spin ? 3 : 2) : -1;
-  const int gn = c.rec ? 2 + c.spin + c.bh : -1;   // N_rec
-  const int gw = c.rec ? gn + 1 : -1;              // weighted_sfr
-  const int gr = c.rec && c.bh ? gn + 2 : -1;      // effective_bhar
+  // the recombination grids (only the 7-grid instantiation runs with recombinations, so the
+  // others compile without this branch)
+  const bool rec = NG == 7 && c.rec;
+  const int gn = rec ? 2 + c.spin + c.bh : -1;     // N_rec
+  const int gw = rec ? gn + 1 : -1;                // weighted_sfr
+  const int gr = rec && c.bh ? gn + 2 : -1;        // effective_bhar
   double acc[FINAL ? HII_NSUM : 1];
 #pragma unroll
   for (int k = 0; k < (FINAL ? HII_NSUM : 1); ++k) acc[k] = 0.0;
@@ -705,18 +708,18 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
 template <int N>
 int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
                  const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
+  // with recombinations (4 to 7 grids) one instantiation reads the count from the batch
+  if (c.rec)
+    return fin ? launch_hii_z3<N, 7, true>(ctx, work, stride, bt, c, s, st, nblocks)
+               : launch_hii_z3<N, 7, false>(ctx, work, stride, bt, c, s, st, nblocks);
   if (ng == 2)
     return fin ? launch_hii_z3<N, 2, true>(ctx, work, stride, bt, c, s, st, nblocks)
                : launch_hii_z3<N, 2, false>(ctx, work, stride, bt, c, s, st, nblocks);
   if (ng == 3)
     return fin ? launch_hii_z3<N, 3, true>(ctx, work, stride, bt, c, s, st, nblocks)
                : launch_hii_z3<N, 3, false>(ctx, work, stride, bt, c, s, st, nblocks);
-  if (ng == 4)
-    return fin ? launch_hii_z3<N, 4, true>(ctx, work, stride, bt, c, s, st, nblocks)
-               : launch_hii_z3<N, 4, false>(ctx, work, stride, bt, c, s, st, nblocks);
-  // 5 to 7 grids (recombinations): one instantiation reads the count from the batch
-  return fin ? launch_hii_z3<N, 7, true>(ctx, work, stride, bt, c, s, st, nblocks)
-             : launch_hii_z3<N, 7, false>(ctx, work, stride, bt, c, s, st, nblocks);
+  return fin ? launch_hii_z3<N, 4, true>(ctx, work, stride, bt, c, s, st, nblocks)
+             : launch_hii_z3<N, 4, false>(ctx, work, stride, bt, c, s, st, nblocks);
 }
 
 // words of packed state per bit kind
