@@ -458,6 +458,45 @@ class HostWorkload:
                     C.byref(wk.hii), C.byref(wk.tb))
 
 
+def time_recombinations(wk, ctx, torch, stream, dev):
+    rg = wk.rg
+    n = wk.n
+    npad, nreal = n * n * 2 * (n // 2 + 1), n ** 3
+    ctx.set_recombination_tables(*wl.rec_stand_in_tables())
+    extra = {"Gamma12": torch.zeros(nreal, device=dev), "N_rec": torch.zeros(npad, device=dev),
+             "residual_xH": torch.zeros(nreal, device=dev), "clumping_factor": torch.zeros(nreal, device=dev),
+             "t_resp": torch.full((nreal,), 1e30, device=dev)}
+    gr = rg.rg_grids.from_buffer_copy(wk.g)
+    for k, v in extra.items():
+        setattr(gr, k, v.data_ptr())
+    pr = rg.rg_params.from_buffer_copy(wk.p)
+    pr.Flag_IncludeRecombinations = 1
+    out = rg.rg_hii_scalars()
+    res = {}
+    for name, p in (("ms", pr), ("ms_without", wk.p)):
+        call = lambda: ctx.call("rg_find_HII_bubbles", C.byref(p), C.byref(wk.s), C.byref(gr), C.byref(out))
+        call()
+        torch.cuda.synchronize(dev)
+        t = []
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            e1.synchronize()
+            t.append(e0.elapsed_time(e1))
+        res[name] = statistics.mean(t)
+        if name == "ms":
+            res["mean_N_rec"] = out.volume_weighted_global_N_rec
+    wk.reset()
+    res["what"] = ("rg_find_HII_bubbles at the workload's size with Flag_IncludeRecombinations (N_rec and "
+                   "weighted_sfr filtered, the recombination closing pass) on stand-in MHR tables; ms_without "
+                   "is the same call without recombinations")
+    del extra
+    return res
+
+
 def timed(torch, stream, fn, reset, warmup, steps):
     for _ in range(warmup):
         reset()
@@ -614,6 +653,11 @@ def run_ours(args, cfg):
         extras["delta_T_velocity_rsd"] = {"ms": statistics.mean(vt),
                                           "what": "rg_delta_T with Flag_IncludePecVelsFor21cm 3 (random velocities)"}
         del vel
+
+    # find_HII_bubbles with inhomogeneous recombinations (stand-in MHR tables): the cost of the
+    # recombination branch next to the same call without it; not part of the metric
+    if not args.no_extras:
+        extras["find_hii_recombinations"] = time_recombinations(wk, ctx, torch, stream, dev)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -167,6 +167,23 @@ class TsInputs:
     stored_fcoll: np.ndarray           # float64 [n_snapshots]
 
 
+def rec_stand_in_tables(nz: int = 200, nt: int = 100, ng: int = 150):
+    """Smooth stand-in MHR recombination tables (lnGamma knots, then ln rate, clumping factor and ln
+    residual xH, each [nz][nt][ng]) with the real tables' sample grid (z = 0.2 i, log10 T =
+    2 + 0.03 j, ln Gamma12 = -10 + 0.1 k as float sums) and ranges (ln rate about -48 to -30,
+    clumping 1 to 5, ln residual xH about -14 to 7).  The MHR integrals themselves are not
+    evaluated: the step only interpolates the tables the caller hands over."""
+    f32 = np.float32
+    knots = np.array([f32(f32(-10.0) + f32(f32(0.1) * f32(i))) for i in range(ng)], np.float64)
+    z = np.arange(nz) * float(f32(0.2))
+    lt = float(f32(2.0)) + np.arange(nt) * float(f32(0.03))
+    Z, T, G = np.meshgrid(z, lt, knots, indexing="ij")
+    RR = -36.3 - 8.0 * np.exp(-(G + 10.0) / 2.5) + 0.15 * (Z - 8.0) - 0.3 * (T - 4.0) + 0.02 * np.sin(1.3 * G)
+    CF = 1.0 + 4.0 / (1.0 + np.exp(-(G + 2.5) / 1.5)) * (1.0 + 0.01 * Z) * (1.0 + 0.05 * (T - 4.0) ** 2)
+    RNH = 6.7 - 1.2 * (G + 10.0) + 0.05 * Z + 0.4 * (T - 4.0) + 0.03 * np.cos(0.7 * G)
+    return knots, RR, CF, RNH
+
+
 def history_scale(zz: np.ndarray, snap: int, h: int) -> float:
     """SFR history amplitude of slot h relative to this snapshot: ((1 + z_h) / (1 + z))^-3."""
     zh = zz[snap - h] if snap - h >= 0 else zz[0]

@@ -95,13 +95,6 @@ class RecTables:
 
 
 def synthetic_tables(nz: int = 200, nt: int = 100, ng: int = 150) -> RecTables:
-    """Smooth stand-in tables with the MHR tables' ranges (ln rate about -48 to -30, clumping 1 to
-    5, ln residual xH about -14 to 7), for parity tests of the interpolation and the branch."""
-    z = np.arange(nz) * Z_DEL
-    lt = T_STA + np.arange(nt) * T_DEL
-    g = knots(ng)
-    Z, T, G = np.meshgrid(z, lt, g, indexing="ij")
-    RR = -36.3 - 8.0 * np.exp(-(G + 10.0) / 2.5) + 0.15 * (Z - 8.0) - 0.3 * (T - 4.0) + 0.02 * np.sin(1.3 * G)
-    CF = 1.0 + 4.0 / (1.0 + np.exp(-(G + 2.5) / 1.5)) * (1.0 + 0.01 * Z) * (1.0 + 0.05 * (T - 4.0) ** 2)
-    RNH = 6.7 - 1.2 * (G + 10.0) + 0.05 * Z + 0.4 * (T - 4.0) + 0.03 * np.cos(0.7 * G)
-    return RecTables(g, RR, CF, RNH)
+    """The stand-in tables of the test inputs (``workloads.rec_stand_in_tables``) with their splines."""
+    import workloads
+    return RecTables(*workloads.rec_stand_in_tables(nz, nt, ng))
