@@ -74,6 +74,10 @@ typedef struct rg_params {
   /* recombinations (Flag_IncludeRecombinations): 1 = the MHR rates at the cell's gas
      temperature, 0 = at 10^4 K (find_HII_bubbles.c:613-619) */
   int Flag_TemperatureDependentRec;
+  /* AGN X-ray channels of ComputeTs (Flag_IncludeAGNXray 1 soft + hard, 2 hard, 3 soft):
+     nu^-alpha indices of the soft (NuXrayThreshold..NuXraySoftCut) and hard
+     (NuXraySoftCut..NuXrayMax) bands (meraxes.h:187-189) */
+  double SpecIndexXrayAGNSoft, SpecIndexXrayAGNHard;
 } rg_params;
 
 /* Fill *p with the values of input/params/defaults.par and the Genesis cosmology/units. */
@@ -121,6 +125,14 @@ typedef struct rg_grids {
   float* residual_xH;
   float* clumping_factor;
   float* t_resp;
+  /* AGN X-ray emissivity (Flag_IncludeAGNXray), padded, in the reference's units (1e10 L_sun per
+     cell): this snapshot's BHXrayEmissivity_soft / _hard and their histories
+     [n_hist][N][N][2(N/2+1)] (bh_xray_histories_soft / _hard), re-weighted per shell like the
+     sfr histories (load_reion_bh_grids, reionization.c) */
+  const float* bh_xray_soft;
+  const float* bh_xray_hard;
+  const float* bh_xray_histories_soft;
+  const float* bh_xray_histories_hard;
 } rg_grids;
 
 /* The snapshot being processed: run_globals.ZZ[] and the snapshot index into it. */
@@ -155,6 +167,7 @@ typedef struct rg_ts_scalars {
   double volume_ave_TS, volume_ave_TK, volume_ave_xe;
   double collapse_fraction, x_e_ave;      /* the stored_fcoll[snapshot] and <x_e> of this step */
   int homogeneous;                        /* 1 when zp >= ReionMaxHeatingRedshift */
+  double volume_ave_Xheat_AGN_soft, volume_ave_Xheat_AGN_hard;   /* Flag_IncludeAGNXray (0 otherwise) */
 } rg_ts_scalars;
 
 typedef struct rg_context rg_context;

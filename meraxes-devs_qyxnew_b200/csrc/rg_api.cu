@@ -269,6 +269,8 @@ int rg_params_default(rg_params* p, int grid_dim, double box_size) {
   p->NuXrayMax = 10000.;
   p->SpecIndexXrayGal = 1.;
   p->Flag_TemperatureDependentRec = 1;   // input/params/defaults.par:19
+  p->SpecIndexXrayAGNSoft = 2.2;          // input/params/defaults.par:67-68
+  p->SpecIndexXrayAGNHard = 1.7;
   return RG_OK;
 }
 
@@ -322,6 +324,7 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->vel_work) cudaFree(ctx->vel_work);
   if (ctx->vel_stage) cudaFree(ctx->vel_stage);
   if (ctx->ngp_bad) cudaFree(ctx->ngp_bad);
+  if (ctx->ts_agn) cudaFree(ctx->ts_agn);
   if (ctx->rec_knots) cudaFree(ctx->rec_knots);
   if (ctx->rec_y) cudaFree(ctx->rec_y);
   if (ctx->rec_c) cudaFree(ctx->rec_c);
@@ -766,8 +769,8 @@ static int compute_ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s,
   const int N = ctx->N;
   if (N < 8 || (N & (N - 1)) != 0)
     return set_error(ctx, RG_EUNSUPPORTED, "ComputeTs needs a power-of-two ReionGridDim");
-  if (p->Flag_IncludeAGNXray)
-    return set_error(ctx, RG_EUNSUPPORTED, "Flag_IncludeAGNXray=1 (AGN X-ray channels) is not implemented");
+  if (p->Flag_IncludeAGNXray < 0 || p->Flag_IncludeAGNXray > 3)
+    return set_error(ctx, RG_EINVAL, "Flag_IncludeAGNXray must be 0, 1, 2 or 3");
   if (p->TsHeatingFilterType < 0 || p->TsHeatingFilterType > 2)
     return set_error(ctx, RG_EINVAL, "TsHeatingFilterType must be 0, 1 or 2");
   if (p->TsNumFilterSteps < 1 || p->TsNumFilterSteps > 1024)
@@ -780,6 +783,11 @@ static int compute_ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s,
   const bool homog = (s->ZZ[s->snapshot] - p->ReionMaxHeatingRedshift) >= -0.0001;
   if (!homog && (!sg->sfr || !sg->xray_luminosity))
     return set_error(ctx, RG_EINVAL, "ComputeTs needs the sfr and xray_luminosity grids");
+  const bool agn_soft = p->Flag_IncludeAGNXray == 1 || p->Flag_IncludeAGNXray == 3;
+  const bool agn_hard = p->Flag_IncludeAGNXray == 1 || p->Flag_IncludeAGNXray == 2;
+  if (!homog && ((agn_soft && (!sg->bh_xray_soft || (sg->n_hist > 0 && !sg->bh_xray_histories_soft))) ||
+                 (agn_hard && (!sg->bh_xray_hard || (sg->n_hist > 0 && !sg->bh_xray_histories_hard)))))
+    return set_error(ctx, RG_EINVAL, "Flag_IncludeAGNXray needs bh_xray_soft/_hard and their histories");
   if ((rc = ensure_tables(ctx, p))) return rc;
   cudaSetDevice(ctx->device);
   rc = ts_snapshot(ctx, p, s, g, out, src_host, stg);

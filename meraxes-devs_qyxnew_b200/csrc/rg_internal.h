@@ -200,6 +200,8 @@ struct rg_context {
   size_t vel_stage_elems = 0;
   int* ngp_bad = nullptr;        // rg_deposit_ngp: count of galaxies below the box
   size_t ngp_bad_elems = 0;
+  float2* ts_agn = nullptr;       // ComputeTs: per-cell AGN heating sums of the two AGN units
+  size_t ts_agn_elems = 0;
   // recombination tables (rg_set_recombination_tables): knots, and per table and (z, T) row the
   // values and the natural-spline coefficients c (half the second derivative), [3][nz*nt][ng]
   double* rec_knots = nullptr;

@@ -1,5 +1,5 @@
-// Spin-temperature step (_ComputeTs, src/core/ComputeTs.c:85-1554) on sm_100a, without the
-// AGN and mini-halo channels.
+// Spin-temperature step (_ComputeTs, src/core/ComputeTs.c:85-1554) on sm_100a, with the AGN
+// X-ray channels (Flag_IncludeAGNXray) and without the mini-halo channels.
 //
 // Inhomogeneous branch, per snapshot:
 //   1. FP64 reductions of the collapse fraction and <x_e> (ComputeTs.c:585-677)
@@ -8,7 +8,8 @@
 //      history slots the shells use); each shell's source is a linear combination of them
 //      (the history re-weighting of :366-478), formed in k-space on load
 //   4. shells in batches: x pass (combination, TsHeatingFilterType window), y pass, z pass
-//      that turns both grids of every shell of the batch into the four per-cell sums of
+//      that turns the grids of every shell (sfr, X-ray, then the AGN soft and / or hard
+//      emissivity) into the four per-cell sums of
 //      evolveInt (X-ray heating, ionisation and Lyman-alpha integrands, stellar Lyman-alpha)
 //      without storing the reference's SMOOTHED_*[nS N^3] arrays
 //   5. per cell, FP64: evolveInt, the Euler step of x_e and T_K, get_Ts, and the FP64 sums
@@ -29,7 +30,7 @@ namespace rg {
 
 constexpr int TS_KB = 8;        // shells per batch
 constexpr int TS_MAXSRC = 4;    // sources combined into one shell
-constexpr int TS_NSUM = 8;      // evolve sums
+constexpr int TS_NSUM = 9;      // evolve sums (7, 8: the AGN heating of the two AGN units)
 constexpr int KSPL = 27;        // knots of the largest kappa table
 
 struct KappaSpline {
@@ -196,6 +197,7 @@ struct TsBatch {
   float cs[TS_KB][TS_MAXSRC];
   int filtered[TS_KB];
   int wrow[TS_KB];
+  int ng;             // grids per shell: sfr, X-ray, then 0 to 2 AGN bands
 };
 
 template <int N>
@@ -238,14 +240,15 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, (x_pass_minb<N>()))
       }
     }
     const int nk = bt.nk[r];
-    for (int g = 0; g < 2; ++g) {
-      cf* dst = work + ((size_t)r * 2 + g) * stride;
+    const int G = bt.ng;
+    for (int g = 0; g < G; ++g) {
+      cf* dst = work + ((size_t)r * G + g) * stride;
       line_fft<N, true>(
           t, xbuf, s_tw,
           [&](int p, int sl) {
             float ax = 0.f, ay = 0.f;
             for (int i = 0; i < nk; ++i) {
-              const cf v = spec[((size_t)bt.ks[r][i] * 2 + g) * stride + col + (size_t)p * N];
+              const cf v = spec[((size_t)bt.ks[r][i] * G + g) * stride + col + (size_t)p * N];
               ax = fmaf(bt.cs[r][i], v.x, ax);
               ay = fmaf(bt.cs[r][i], v.y, ay);
             }
@@ -333,6 +336,10 @@ struct TsShellCoef {
   float Q[3][x_int_NXHII];
   float cstar;
   float pad;
+  // AGN units j = 0, 1 (the bands in use, soft first): max(grid, 0) x (PA + dx QA), with the
+  // ratio of the band's prefactor to the galaxies' folded in so the terms join the same sums
+  float PA[2][3][x_int_NXHII];
+  float QA[2][3][x_int_NXHII];
 };
 
 struct TsZev {
@@ -387,11 +394,13 @@ __device__ __forceinline__ cf ts_tile_input(const cf* tile, int q, int p) {
   return cf{A.x + B.y, B.x - A.y};
 }
 
-template <int N>
+// G grids per shell: 0 sfr, 1 X-ray, 2 and 3 the AGN bands in use (their per-cell heating
+// terms also go to agn_heat, for the AGN heating averages)
+template <int N, int G>
 __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
     k_ts_zsum(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw,
               const TsShellCoef* __restrict__ gco, TsZev zv, const float* __restrict__ xe_prev,
-              float4* __restrict__ sums) {
+              float4* __restrict__ sums, float2* __restrict__ agn_heat) {
   using Z = TsZ<N>;
   using PL = typename Z::PL;
   constexpr int Q = Z::Q, V = Z::V;
@@ -432,22 +441,45 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
     dxe[sl] = (float)(xc - (double)xm);
   }
   float a_heat[V], a_ion[V], a_lya[V], a_star[V];
+  float a_agn0[G > 2 ? V : 1], a_agn1[G > 3 ? V : 1];
 #pragma unroll
   for (int sl = 0; sl < V; ++sl) a_heat[sl] = a_ion[sl] = a_lya[sl] = a_star[sl] = 0.f;
+#pragma unroll
+  for (int sl = 0; sl < (G > 2 ? V : 1); ++sl) a_agn0[sl] = 0.f;
+#pragma unroll
+  for (int sl = 0; sl < (G > 3 ? V : 1); ++sl) a_agn1[sl] = 0.f;
   auto addr = [&](int p) { return line_addr_r0<Z::R0, Q>(p, threadIdx.x % Q); };
-  // units u = 2 (r / 2) + g: the pair of shells (r, r + 1), grid g (0 sfr, 1 X-ray); the tile of
-  // unit u + 1 is copied while unit u is transformed
+  // units u = G (r / 2) + g: the pair of shells (r, r + 1), grid g; the tile of unit u + 1 is
+  // copied while unit u is transformed
   const int y0 = blockIdx.x * Q, q = threadIdx.x % Q;
   auto unit_src = [&](int u, int which) -> const cf* {
-    const int r = 2 * (u >> 1) + which, g = u & 1;
-    return r < zv.nS ? work + ((size_t)r * 2 + g) * stride : nullptr;
+    const int r = 2 * (u / G) + which, g = u % G;
+    return r < zv.nS ? work + ((size_t)r * G + g) * stride : nullptr;
   };
-  const int nunits = 2 * ((zv.nS + 1) / 2);
+  const int nunits = G * ((zv.nS + 1) / 2);
   if (nunits > 0) ts_tile_issue<N, Q>(tiles, unit_src(0, 0), unit_src(0, 1), x, y0, Z::NTH);
   cp_async_commit();
+  // an AGN unit j: clamped at 0 (ComputeTs.c:615-630), its own band tables
+  auto agn_unit = [&](const cf* tile, int j, float (&ah)[G > 2 ? V : 1]) {
+    line_fft_p<PL, true>(
+        t, xbuf, s_tw, [&](int p, int) { return ts_tile_input<N, Q>(tile, q, p); }, addr,
+        [&](int, cf v, int sl) {
+          const int lo = (int)((lopack >> (4 * sl)) & 15u);
+          const float d = dxe[sl];
+          const float vx = fmaxf(v.x, 0.f), vy = fmaxf(v.y, 0.f);
+          const float h = vx * fmaf(d, sc[0].QA[j][0][lo], sc[0].PA[j][0][lo]) +
+                          vy * fmaf(d, sc[1].QA[j][0][lo], sc[1].PA[j][0][lo]);
+          a_heat[sl] += h;
+          ah[sl] += h;
+          a_ion[sl] += vx * fmaf(d, sc[0].QA[j][1][lo], sc[0].PA[j][1][lo]) +
+                       vy * fmaf(d, sc[1].QA[j][1][lo], sc[1].PA[j][1][lo]);
+          a_lya[sl] += vx * fmaf(d, sc[0].QA[j][2][lo], sc[0].PA[j][2][lo]) +
+                       vy * fmaf(d, sc[1].QA[j][2][lo], sc[1].PA[j][2][lo]);
+        });
+  };
   for (int u = 0; u < nunits; ++u) {
-    const int r = 2 * (u >> 1);
-    if ((u & 1) == 0) {
+    const int r = 2 * (u / G), g = u % G;
+    if (g == 0) {
       __syncthreads();  // readers of the previous pair's coefficients are done
       const bool two = r + 1 < zv.nS;
       const int* src = reinterpret_cast<const int*>(gco + r);
@@ -463,13 +495,13 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
     cp_async_wait<1>();
     __syncthreads();  // unit u's tile (and the pair's coefficients) are visible to every thread
     const cf* tile = tiles + (u & 1) * Z::tile_elems();
-    if ((u & 1) == 0) {
+    if (g == 0) {
       // sfr: stellar Lyman-alpha sum, SFR clamped at 0 (ComputeTs.c:700)
       const float c0 = sc[0].cstar, c1 = sc[1].cstar;
       line_fft_p<PL, true>(
           t, xbuf, s_tw, [&](int p, int) { return ts_tile_input<N, Q>(tile, q, p); }, addr,
           [&](int, cf v, int sl) { a_star[sl] += fmaxf(v.x, 0.f) * c0 + fmaxf(v.y, 0.f) * c1; });
-    } else {
+    } else if (g == 1) {
       // X-ray: heating, ionisation and Lyman-alpha integrands, not clamped
       line_fft_p<PL, true>(
           t, xbuf, s_tw, [&](int p, int) { return ts_tile_input<N, Q>(tile, q, p); }, addr,
@@ -480,17 +512,27 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
             a_ion[sl] += v.x * fmaf(d, sc[0].Q[1][lo], sc[0].P[1][lo]) + v.y * fmaf(d, sc[1].Q[1][lo], sc[1].P[1][lo]);
             a_lya[sl] += v.x * fmaf(d, sc[0].Q[2][lo], sc[0].P[2][lo]) + v.y * fmaf(d, sc[1].Q[2][lo], sc[1].P[2][lo]);
           });
+    } else if constexpr (G > 2) {
+      if (g == 2) {
+        agn_unit(tile, 0, a_agn0);
+      } else if constexpr (G > 3) {
+        agn_unit(tile, 1, a_agn1);
+      }
     }
     __syncthreads();  // the tile is consumed before unit u + 2 refills it
   }
 #pragma unroll
-  for (int sl = 0; sl < V; ++sl)
-    sums[row * N + last_pos<PL>(t, sl)] = make_float4(a_heat[sl], a_ion[sl], a_lya[sl], a_star[sl]);
+  for (int sl = 0; sl < V; ++sl) {
+    const size_t ic = row * N + last_pos<PL>(t, sl);
+    sums[ic] = make_float4(a_heat[sl], a_ion[sl], a_lya[sl], a_star[sl]);
+    if constexpr (G > 2) agn_heat[ic] = make_float2(a_agn0[sl], G > 3 ? a_agn1[G > 3 ? sl : 0] : 0.f);
+  }
 }
 
 // the per-cell update (ComputeTs.c:1171-1407) from the shell sums; sums == nullptr: no light
 __global__ void __launch_bounds__(256) k_ts_evolve(const TsDev* __restrict__ gC, TsEvolve e, double4 inv_scale, int n,
                                                    const float4* __restrict__ sums,
+                                                   const float2* __restrict__ agn_heat,
                                                    const float* __restrict__ deltax, float* __restrict__ xe_prev,
                                                    float* __restrict__ xe_box, float* __restrict__ Tk,
                                                    float* __restrict__ TS, double* __restrict__ partials,
@@ -520,7 +562,15 @@ __global__ void __launch_bounds__(256) k_ts_evolve(const TsDev* __restrict__ gC,
         sm[3] = (double)v.w * inv_scale.w;
       }
       float xn, tk, ts;
-      evolve_cell(C, e, __ldg(deltax + ip), xe_prev[ip], Tk[ir], sm, &xn, &tk, &ts, acc, &nc);
+      const float xe0 = xe_prev[ip];
+      if (agn_heat) {
+        // the AGN heating terms of dT_K/dz (XRayHeatingFunctions.c:1519-1520) for their averages
+        const float2 a = __ldg(agn_heat + ir);
+        const double f = inv_scale.x * e.const_zp * e.heat_conv / (1.0 + (double)xe0);
+        acc[7] += (double)a.x * f;
+        acc[8] += (double)a.y * f;
+      }
+      evolve_cell(C, e, __ldg(deltax + ip), xe0, Tk[ir], sm, &xn, &tk, &ts, acc, &nc);
       xe_prev[ip] = xn;
       xe_box[ip] = xn;
       Tk[ir] = tk;
@@ -586,7 +636,7 @@ static void fill_spline(const CubicSpline& sp, const std::vector<double>& lx, co
   }
 }
 
-// x and y passes of a batch of shells: work_base + (j * 2 + g) * stride, j < bt.nr
+// x and y passes of a batch of shells: work_base + (j * bt.ng + g) * stride, j < bt.nr
 template <int N>
 static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
                         const float* wtab, int wpitch, const int* wcut, cudaStream_t st) {
@@ -601,34 +651,43 @@ static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t s
   k_ts_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, smx, st>>>(spec, stride, work_base, bt, wtab, wpitch, wcut, tw);
   double src_reads = 0;
   for (int r = 0; r < bt.nr; ++r) src_reads += bt.nk[r];
-  prof_end(ctx, 2 * 8.0 * nzc * (src_reads + bt.nr), st);
+  prof_end(ctx, bt.ng * 8.0 * nzc * (src_reads + bt.nr), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   const size_t smy = sizeof(cf) * (N + (size_t)C::BY * C::PITCH_P);
   RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_pass_y<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
   prof_begin(ctx, "ts_y_c2c", st);
-  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, 2 * bt.nr), C::T * C::BY, smy, st>>>(work_base, stride, tw);
-  prof_end(ctx, 2 * bt.nr * 16.0 * nzc, st);
+  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, bt.ng * bt.nr), C::T * C::BY, smy, st>>>(work_base, stride, tw);
+  prof_end(ctx, bt.ng * bt.nr * 16.0 * nzc, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 
 // the z pass over all nS shells: per-cell shell sums
-template <int N>
-static int launch_ts_zsum(rg_context* ctx, const cf* work, size_t stride, const TsShellCoef* d_co, const TsZev& zv,
-                          const float* xe_prev, float4* sums, cudaStream_t st) {
+template <int N, int G>
+static int launch_ts_zsum_g(rg_context* ctx, const cf* work, size_t stride, const TsShellCoef* d_co, const TsZev& zv,
+                            const float* xe_prev, float4* sums, float2* agn_heat, cudaStream_t st) {
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
   using Z = TsZ<N>;
   const double n3 = (double)N * N * N, nzc = (double)(N / 2 + 1) * N * N;
   const size_t smz = Z::smem();
-  RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_zsum<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+  RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_zsum<N, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
   prof_begin(ctx, "ts_z_c2r_sums", st);
-  k_ts_zsum<N><<<dim3(N / Z::Q, N), Z::NTH, smz, st>>>(work, stride, tw, d_co, zv, xe_prev, sums);
-  // Hermitian halves of both grids of every shell, x_e read, four float sums written
-  prof_end(ctx, zv.nS * 2 * 8.0 * nzc + 4.0 * n3 + 16.0 * n3, st);
+  k_ts_zsum<N, G><<<dim3(N / Z::Q, N), Z::NTH, smz, st>>>(work, stride, tw, d_co, zv, xe_prev, sums, agn_heat);
+  // Hermitian halves of the G grids of every shell, x_e read, four float sums (and the AGN
+  // heating pair) written
+  prof_end(ctx, zv.nS * G * 8.0 * nzc + 4.0 * n3 + 16.0 * n3 + (G > 2 ? 8.0 * n3 : 0.0), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
+}
+
+template <int N>
+static int launch_ts_zsum(rg_context* ctx, const cf* work, size_t stride, int ng, const TsShellCoef* d_co,
+                          const TsZev& zv, const float* xe_prev, float4* sums, float2* agn_heat, cudaStream_t st) {
+  if (ng == 2) return launch_ts_zsum_g<N, 2>(ctx, work, stride, d_co, zv, xe_prev, sums, nullptr, st);
+  if (ng == 3) return launch_ts_zsum_g<N, 3>(ctx, work, stride, d_co, zv, xe_prev, sums, agn_heat, st);
+  return launch_ts_zsum_g<N, 4>(ctx, work, stride, d_co, zv, xe_prev, sums, agn_heat, st);
 }
 
 #define RG_TS_DISPATCH(n, call)                                                           \
@@ -648,9 +707,9 @@ static int ts_xy(rg_context* ctx, int n, const cf* spec, cf* work_base, size_t s
   RG_TS_DISPATCH(n, launch_ts_xy<NN>(ctx, spec, work_base, stride, bt, wtab, wpitch, wcut, st));
 }
 
-static int ts_zsum(rg_context* ctx, int n, const cf* work, size_t stride, const TsShellCoef* d_co, const TsZev& zv,
-                   const float* xe_prev, float4* sums, cudaStream_t st) {
-  RG_TS_DISPATCH(n, launch_ts_zsum<NN>(ctx, work, stride, d_co, zv, xe_prev, sums, st));
+static int ts_zsum(rg_context* ctx, int n, const cf* work, size_t stride, int ng, const TsShellCoef* d_co,
+                   const TsZev& zv, const float* xe_prev, float4* sums, float2* agn_heat, cudaStream_t st) {
+  RG_TS_DISPATCH(n, launch_ts_zsum<NN>(ctx, work, stride, ng, d_co, zv, xe_prev, sums, agn_heat, st));
 }
 
 static double pow2_scale(double maxabs) {
@@ -678,6 +737,12 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double box_size = p->BoxSize / p->Hubble_h;  // Mpc
   const double pixel_volume = std::pow(box_size / (double)N, 3);
   std::memset(out, 0, sizeof(*out));
+  // grids per shell: sfr, X-ray, then the AGN bands in use (0 soft, 1 hard)
+  const int agn_flag = p->Flag_IncludeAGNXray;
+  int bands[2] = {-1, -1}, nagn = 0;
+  if (agn_flag == 1 || agn_flag == 3) bands[nagn++] = 0;
+  if (agn_flag == 1 || agn_flag == 2) bands[nagn++] = 1;
+  const int G = 2 + nagn;
 
   // device constants: kappa splines and number densities
   TsDev hc;
@@ -739,6 +804,8 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       out->volume_ave_xalpha = S[1] / nn;
       out->volume_ave_Xheat = S[2] / nn;
       out->volume_ave_Xion = S[3] / nn;
+      for (int j = 0; j < nagn; ++j)
+        (bands[j] ? out->volume_ave_Xheat_AGN_hard : out->volume_ave_Xheat_AGN_soft) = S[7 + j] / nn;
     }
     out->volume_ave_TS = S[4] / nn;
     out->volume_ave_TK = S[5] / nn;
@@ -805,18 +872,24 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       if (nk > TS_MAXSRC) return set_error(ctx, RG_EUNSUPPORTED, "a shell combines more than 4 history snapshots");
     }
     const int nused = std::max(1, (int)used.size());
-    if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * 2 * nused))) return rc;
-    // every shell's filtered grids stay in HBM until the fused z pass (2 nS spectra)
-    if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * 2 * nS))) return rc;
-    // source grid `which` (0 sfr, 1 xray) of source k, on the device
+    if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * G * nused))) return rc;
+    // every shell's filtered grids stay in HBM until the fused z pass (G nS spectra)
+    if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * G * nS))) return rc;
+    // source grid `which` (0 sfr, 1 xray, 2 + j AGN band bands[j]) of source k, on the device
+    // (the AGN histories are re-weighted like the sfr ones, load_reion_bh_grids)
     const rg_grids* sg = src_host ? src_host : g;
     auto src_grid = [&](int k, int which) -> const float* {
+      if (which >= 2) {
+        const bool hard = bands[which - 2] == 1;
+        if (k == 0) return hard ? sg->bh_xray_hard : sg->bh_xray_soft;
+        return (hard ? sg->bh_xray_histories_hard : sg->bh_xray_histories_soft) + (size_t)(k - 1) * npad;
+      }
       if (k == 0) return which ? sg->xray_luminosity : sg->sfr;
       return (which ? sg->xray_luminosity_histories : sg->sfr_histories) + (size_t)(k - 1) * npad;
     };
-    if (src_host && (rc = ensure_device(ctx, &ctx->ts_stage, &ctx->ts_stage_elems, npad * 2 * used.size()))) return rc;
+    if (src_host && (rc = ensure_device(ctx, &ctx->ts_stage, &ctx->ts_stage_elems, npad * G * used.size()))) return rc;
     auto dev_grid = [&](size_t j, int which) -> const float* {
-      return src_host ? ctx->ts_stage + (j * 2 + which) * npad : src_grid(used[j], which);
+      return src_host ? ctx->ts_stage + (j * G + which) * npad : src_grid(used[j], which);
     };
     // window rows for the shells (filter() takes BoxSize in Mpc/h and R in Mpc, ComputeTs.c:532)
     const int n2max = 3 * (N / 2) * (N / 2);
@@ -833,7 +906,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     // is in order of first use), then its x and y passes into work[r][g].  From host arrays,
     // each group of sources is copied on the copy stream and its transform waits for the copy,
     // so the copies of later sources overlap the passes of earlier batches.
-    size_t next_slot = 0;   // used[0, next_slot) are transformed into spec[slot * 2 + g]
+    size_t next_slot = 0;   // used[0, next_slot) are transformed into spec[slot * G + g]
     for (int r0 = 0; r0 < nS; r0 += TS_KB) {
       const int cnt = std::min(TS_KB, nS - r0);
       size_t need = next_slot;
@@ -841,29 +914,28 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
         for (int k = 0; k < sh.nsrc; ++k)
           if (sh.coef[(size_t)r * sh.nsrc + k] != 0.f) need = std::max(need, (size_t)slot_of[k] + 1);
       while (next_slot < need) {
-        const size_t end = std::min(need, next_slot + 4);
+        const size_t end = std::min(need, next_slot + (size_t)(MAXG / G));
         if (src_host) {
           for (size_t j = next_slot; j < end; ++j)
-            for (int which = 0; which < 2; ++which)
-              RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ts_stage + (j * 2 + which) * npad, src_grid(used[j], which),
+            for (int which = 0; which < G; ++which)
+              RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->ts_stage + (j * G + which) * npad, src_grid(used[j], which),
                                                sizeof(float) * npad, cudaMemcpyHostToDevice, ctx->copy_stream));
           cudaEvent_t e;
           if ((rc = stage_record(ctx, 4 + next_slot, ctx->copy_stream, &e))) return rc;
           if ((rc = stage_wait(ctx, e, st))) return rc;
         }
-        const float* srcs[8];
+        const float* srcs[MAXG];
         int ng = 0;
-        for (size_t j = next_slot; j < end; ++j) {
-          srcs[ng++] = dev_grid(j, 0);
-          srcs[ng++] = dev_grid(j, 1);
-        }
-        if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec + nc * 2 * next_slot, nc, 1.0 / std::pow((double)N, 3), st)))
+        for (size_t j = next_slot; j < end; ++j)
+          for (int which = 0; which < G; ++which) srcs[ng++] = dev_grid(j, which);
+        if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec + nc * G * next_slot, nc, 1.0 / std::pow((double)N, 3), st)))
           return rc;
         next_slot = end;
       }
       TsBatch bt;
       std::memset(&bt, 0, sizeof(bt));
       bt.nr = cnt;
+      bt.ng = G;
       for (int j = 0; j < cnt; ++j) {
         const int r = r0 + j;
         int nk = 0;
@@ -879,7 +951,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
         bt.filtered[j] = r > 0;  // no filter on the first shell (ComputeTs.c:529)
         bt.wrow[j] = r;
       }
-      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * 2 * nc, nc, bt, ctx->wtab, n2max + 1, wcut, st)))
+      if ((rc = ts_xy(ctx, N, ctx->spec, ctx->work + (size_t)r0 * G * nc, nc, bt, ctx->wtab, n2max + 1, wcut, st)))
         return rc;
     }
     if ((rc = kick())) return rc;
@@ -919,6 +991,31 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       cs[r] = convS * opzf2 * (1 + sh.zpp[r]) * tb.sum_lyn[r] * a;
       maxk[3] = std::max(maxk[3], std::fabs(cs[r]));
     }
+    // AGN bands: XAGN_R = max(bh, 0) 1e10 L_sun / pv UL^-3 (ComputeTs.c:615-630), the band's
+    // (1+zpp)^-alpha and tables, and const_zp_AGN / const_zp_GAL so the terms share the
+    // galaxies' prefactor in the update kernel (XRayHeatingFunctions.c:1420-1470)
+    const double convA = 1e10 * SOLAR_LUM / pixel_volume * std::pow(p->UnitLength_in_cm, -3.0);
+    std::vector<double> PAd((size_t)nS * 2 * 3 * x_int_NXHII, 0.0), QAd(PAd.size(), 0.0);
+    for (int j = 0; j < nagn; ++j) {
+      const int b = bands[j];
+      const double alpha_b = b ? p->SpecIndexXrayAGNHard : p->SpecIndexXrayAGNSoft;
+      const double ratio = pf.const_zp_prefactor_AGN[b] / pf.const_zp_prefactor_GAL;
+      for (int r = 0; r < nS; ++r) {
+        const double a = sh.dt_dzpp[r] * sh.dzpp[r] * convA * std::pow(1 + sh.zpp[r], -alpha_b) * ratio;
+        for (int kind = 0; kind < 3; ++kind) {
+          const std::vector<double>& tb_k = tb.agn[b][kind];
+          for (int m = 0; m < x_int_NXHII; ++m) {
+            const double t_lo = tb_k[(size_t)m * nS + r];
+            const double t_hi = m + 1 < x_int_NXHII ? tb_k[(size_t)(m + 1) * nS + r] : t_lo;
+            const double slope = m + 1 < x_int_NXHII ? (t_hi - t_lo) / ((double)X[m + 1] - (double)X[m]) : 0.0;
+            const size_t o = (((size_t)r * 2 + j) * 3 + kind) * x_int_NXHII + m;
+            PAd[o] = a * t_lo;
+            QAd[o] = a * slope;
+            maxk[kind] = std::max({maxk[kind], std::fabs(a * t_lo), std::fabs(a * t_hi)});
+          }
+        }
+      }
+    }
     // FP32 sums over the shells: scale each sum by a power of two that brings its largest
     // per-shell coefficient near 1 (values of order 1e-30 would lose range in float)
     double scale[4];
@@ -935,11 +1032,21 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
           hco[r].Q[kind][m] = (float)(Qd[((size_t)r * 3 + kind) * x_int_NXHII + m] * scale[kind]);
         }
       hco[r].cstar = (float)(cs[r] * scale[3]);
+      for (int j = 0; j < nagn; ++j)
+        for (int kind = 0; kind < 3; ++kind)
+          for (int m = 0; m < x_int_NXHII; ++m) {
+            const size_t o = (((size_t)r * 2 + j) * 3 + kind) * x_int_NXHII + m;
+            hco[r].PA[j][kind][m] = (float)(PAd[o] * scale[kind]);
+            hco[r].QA[j][kind][m] = (float)(QAd[o] * scale[kind]);
+          }
     }
     RG_CUDA_TRY(ctx, cudaMemcpyAsync(d_co, hco.data(), sizeof(TsShellCoef) * (nS + 1), cudaMemcpyHostToDevice, st));
     zv.nS = nS;
     if ((rc = ensure_device(ctx, &ctx->ts_sums, &ctx->ts_sums_elems, n3))) return rc;
-    if ((rc = ts_zsum(ctx, N, ctx->work, nc, d_co, zv, g->x_e_box_prev, ctx->ts_sums, st))) return rc;
+    if (nagn && (rc = ensure_device(ctx, &ctx->ts_agn, &ctx->ts_agn_elems, n3))) return rc;
+    if ((rc = ts_zsum(ctx, N, ctx->work, nc, G, d_co, zv, g->x_e_box_prev, ctx->ts_sums, nagn ? ctx->ts_agn : nullptr,
+                      st)))
+      return rc;
     RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // hco outlives the copy
   }
 
@@ -957,7 +1064,8 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double4 inv = make_double4(zv.inv_scale[0], zv.inv_scale[1], zv.inv_scale[2], zv.inv_scale[3]);
   prof_begin(ctx, "ts_evolve", st);
   if ((rc = stage_wait(ctx, stg->closing, st))) return rc;
-  k_ts_evolve<<<nblk, 256, 0, st>>>(d_hc, e, inv, N, no_light ? nullptr : ctx->ts_sums, g->deltax, g->x_e_box_prev,
+  k_ts_evolve<<<nblk, 256, 0, st>>>(d_hc, e, inv, N, no_light ? nullptr : ctx->ts_sums,
+                                     (no_light || !nagn) ? nullptr : ctx->ts_agn, g->deltax, g->x_e_box_prev,
                                      g->x_e_box, g->Tk_box, g->TS_box, partials, d_nonconv);
   prof_end(ctx, (double)n3 * (16 + 4 + 4 + 4 + 4 + 4 + 4 + 4), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());

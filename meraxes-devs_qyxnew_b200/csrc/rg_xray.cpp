@@ -541,9 +541,9 @@ int ts_tables(const rg_params* p, const Tables& t, const TsShells& sh, double zp
     return brent_root([&](double nu) { return tauX(nu, x_e, zpv, zpp) - 1; }, HeI_NUIONIZATION, 1e6 * NU_over_EV, 0,
                       0.02, 100, &st);
   };
-  const double thresh = p->NuXrayThreshold, alpha = p->SpecIndexXrayGal;
-  // integrate_over_nu (XRayHeatingFunctions.c:742-856)
-  auto integrate_over_nu = [&](double local_x_e, double lo, double hi, int FLAG) {
+  const double thresh = p->NuXrayThreshold;
+  // integrate_over_nu (XRayHeatingFunctions.c:742-856) for the spectral index alpha
+  auto integrate_over_nu = [&](double local_x_e, double lo, double hi, int FLAG, double alpha) {
     if (lo >= hi) return 0.0;
     const float xf = (float)local_x_e;
     auto pw = [&](double nu) { return std::pow(nu / (thresh * NU_over_EV), -alpha - 1); };
@@ -599,13 +599,37 @@ int ts_tables(const rg_params* p, const Tables& t, const TsShells& sh, double zp
     ntone[R_ct] = nu_tau_one_zpp;
     const double lower = std::fmax(nu_tau_one_zpp, thresh * NU_over_EV);
     const double upper = p->NuXrayMax * NU_over_EV;
+    const double alpha = p->SpecIndexXrayGal;
     for (int x_e_ct = 0; x_e_ct < x_int_NXHII; x_e_ct++) {
       const double xe = t.x_int_XHII[x_e_ct];
-      out->heat[(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lower, upper, 0);
-      out->ion[(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lower, upper, 1);
-      out->lya[(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lower, upper, 2);
+      out->heat[(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lower, upper, 0, alpha);
+      out->ion[(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lower, upper, 1, alpha);
+      out->lya[(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lower, upper, 2, alpha);
+    }
+    // AGN bands: limits redshifted from zpp to zp (ComputeTs.c:834-897)
+    const double zf = (1. + zp) / (1. + zpp);
+    for (int b = 0; b < 2; ++b) {
+      if (out->agn[b][0].empty()) continue;
+      const double lo_b = std::fmax(nu_tau_one_zpp, (b ? p->NuXraySoftCut : thresh) * NU_over_EV * zf);
+      const double hi_b = (b ? p->NuXrayMax : p->NuXraySoftCut) * NU_over_EV * zf;
+      const double a_b = b ? p->SpecIndexXrayAGNHard : p->SpecIndexXrayAGNSoft;
+      for (int x_e_ct = 0; x_e_ct < x_int_NXHII; x_e_ct++) {
+        const double xe = t.x_int_XHII[x_e_ct];
+        for (int kind = 0; kind < 3; ++kind)
+          out->agn[b][kind][(size_t)x_e_ct * nS + R_ct] = integrate_over_nu(xe, lo_b, hi_b, kind, a_b);
+      }
     }
   };
+  const int agn_flag = p->Flag_IncludeAGNXray;
+  for (int b = 0; b < 2; ++b) {
+    const bool on = b == 0 ? (agn_flag == 1 || agn_flag == 3) : (agn_flag == 1 || agn_flag == 2);
+    for (int kind = 0; kind < 3; ++kind) {
+      if (on)
+        out->agn[b][kind].assign((size_t)x_int_NXHII * nS, 0);
+      else
+        out->agn[b][kind].clear();
+    }
+  }
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const int nth = (int)std::min<unsigned>(hw, (unsigned)nS);
   std::vector<std::thread> pool;
@@ -680,6 +704,24 @@ TsPrefactors ts_prefactors(const rg_params* p, double zp) {
   f.Luminosity_conversion_factor_GAL = L;
   f.const_zp_prefactor_GAL =
       L / (p->NuXrayThreshold * NU_over_EV) * SPEED_OF_LIGHT * std::pow(1 + zp, p->SpecIndexXrayGal + 3);
+  // AGN bands: soft NuXrayThreshold..NuXraySoftCut, hard NuXraySoftCut..NuXrayMax, the spectrum
+  // normalised at NuXrayThreshold (ComputeTs.c:1049-1081,1116-1131)
+  for (int b = 0; b < 2; ++b) {
+    const double a = b ? p->SpecIndexXrayAGNHard : p->SpecIndexXrayAGNSoft;
+    const double nlo = b ? p->NuXraySoftCut : p->NuXrayThreshold, nhi = b ? p->NuXrayMax : p->NuXraySoftCut;
+    double La;
+    if (std::fabs(a - 1.0) < (double)REL_TOL) {
+      La = (p->NuXrayThreshold * NU_over_EV) * std::log(nhi / nlo);
+      La = 1.0 / La;
+    } else {
+      La = std::pow(nhi * NU_over_EV, 1.0 - a) - std::pow(nlo * NU_over_EV, 1.0 - a);
+      La = 1.0 / La;
+      La *= std::pow(p->NuXrayThreshold * NU_over_EV, -a) * (1.0 - a);
+    }
+    La /= PLANCK;
+    f.const_zp_prefactor_AGN[b] =
+        La / (p->NuXrayThreshold * NU_over_EV) * SPEED_OF_LIGHT * std::pow(1.0 + zp, a + 3.0);
+  }
   return f;
 }
 

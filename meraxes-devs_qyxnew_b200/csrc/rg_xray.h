@@ -66,6 +66,9 @@ TsShells ts_shells(const rg_params* p, const double* ZZ, int n_snap, int snapsho
 // (ComputeTs.c:761-808) and the Lyman-n sums with the kink correction (:900-1011).
 struct TsTables {
   std::vector<double> heat, ion, lya;   // [14][nS]
+  // AGN X-ray bands (Flag_IncludeAGNXray), [band 0 soft, 1 hard][kind heat, ion, lya][14][nS]
+  // (ComputeTs.c:834-897); empty for a band that is off
+  std::vector<double> agn[2][3];
   std::vector<double> sum_lyn;          // [nS]
   double nu_tau_one_min = 0, nu_tau_one_max = 0;
 };
@@ -76,6 +79,7 @@ int ts_tables(const rg_params* p, const Tables& t, const TsShells& sh, double zp
 // Per-snapshot prefactors (ComputeTs.c:1014-1109)
 struct TsPrefactors {
   double growth_factor_zp, dgrowth_factor_dzp, dt_dzp, const_zp_prefactor_GAL, Luminosity_conversion_factor_GAL;
+  double const_zp_prefactor_AGN[2];   // soft, hard (ComputeTs.c:1049-1081,1116-1131)
 };
 TsPrefactors ts_prefactors(const rg_params* p, double zp);
 

@@ -42,6 +42,7 @@ class rg_params(C.Structure):
         ("TablesForXHeatingDir", C.c_char_p),
         ("TreesID", C.c_int),
         ("Flag_TemperatureDependentRec", C.c_int),
+        ("SpecIndexXrayAGNSoft", C.c_double), ("SpecIndexXrayAGNHard", C.c_double),
     ]
 
 
@@ -62,6 +63,8 @@ class rg_grids(C.Structure):
         ("vel", C.c_void_p),
         ("Gamma12", C.c_void_p), ("N_rec", C.c_void_p), ("residual_xH", C.c_void_p),
         ("clumping_factor", C.c_void_p), ("t_resp", C.c_void_p),
+        ("bh_xray_soft", C.c_void_p), ("bh_xray_hard", C.c_void_p), ("bh_xray_histories_soft", C.c_void_p),
+        ("bh_xray_histories_hard", C.c_void_p),
     ]
 
 
@@ -88,7 +91,7 @@ class rg_ts_scalars(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "volume_ave_J_alpha", "volume_ave_xalpha", "volume_ave_Xheat", "volume_ave_Xion",
         "volume_ave_TS", "volume_ave_TK", "volume_ave_xe", "collapse_fraction", "x_e_ave")] + [
-        ("homogeneous", C.c_int)]
+        ("homogeneous", C.c_int), ("volume_ave_Xheat_AGN_soft", C.c_double), ("volume_ave_Xheat_AGN_hard", C.c_double)]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}

@@ -95,6 +95,8 @@ class Params:
     NuXrayMax: float = 10000.0
     SpecIndexXrayGal: float = 1.0
     Flag_TemperatureDependentRec: int = 1
+    SpecIndexXrayAGNSoft: float = 2.2
+    SpecIndexXrayAGNHard: float = 1.7
 
 
 @dataclasses.dataclass

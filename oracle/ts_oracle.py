@@ -64,6 +64,7 @@ MAX_TK = f32(5e4)
 MIN_TK = f32(0.1)
 R_XLy_MAX = 500.0
 XRAY_LUMINOSITY_UNIT = 1.0e40
+SOLAR_LUM = 3.826e33
 NSPEC_MAX = 23
 L_FACTOR = ro.L_FACTOR
 DBL_EPSILON = np.finfo(np.float64).eps
@@ -418,8 +419,11 @@ class Shells:
     pass
 
 
-def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xray_hist, want_grids=True):
-    """Returns (Shells, per-shell list of (sfr, xray) float32 grids or None)."""
+def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xray_hist, want_grids=True,
+                       extra=()):
+    """Returns (Shells, per-shell list of (sfr, xray, *extra) float32 grids or None).  ``extra`` holds
+    (grid, histories) pairs re-weighted like the sfr grids: the AGN emissivity bands
+    (load_reion_bh_grids)."""
     cm = Cosmo(p)
     nS = p.TsNumFilterSteps
     box = p.BoxSize / p.Hubble_h
@@ -434,29 +438,26 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
     sh.R = np.zeros(nS)
     sh.zpp_edge = np.zeros(nS)
     scb = np.zeros(nS, np.int64)
-    cur_s = None if not want_grids else sfr.astype(f32).copy()
-    cur_x = None if not want_grids else xray.astype(f32).copy()
+    hists = [sfr_hist, xray_hist] + [e[1] for e in extra]
+    cur = None if not want_grids else [a.astype(f32).copy() for a in [sfr, xray] + [e[0] for e in extra]]
     grids = []
 
     def load(idx, weight, new_load):
-        nonlocal cur_s, cur_x
+        nonlocal cur
         if idx < 0 or idx >= len(sfr_hist):
             raise ValueError("history slot %d missing" % idx)
         if not want_grids:
             return
         w = f32(weight)
         if new_load:
-            cur_s = (sfr_hist[idx].astype(f32) * w).astype(f32)
-            cur_x = (xray_hist[idx].astype(f32) * w).astype(f32)
+            cur = [(h[idx].astype(f32) * w).astype(f32) for h in hists]
         else:
-            cur_s = (cur_s + (sfr_hist[idx].astype(f32) * w).astype(f32)).astype(f32)
-            cur_x = (cur_x + (xray_hist[idx].astype(f32) * w).astype(f32)).astype(f32)
+            cur = [(c + (h[idx].astype(f32) * w).astype(f32)).astype(f32) for c, h in zip(cur, hists)]
 
     def clear():
-        nonlocal cur_s, cur_x
+        nonlocal cur
         if want_grids:
-            cur_s = np.zeros_like(cur_s)
-            cur_x = np.zeros_like(cur_x)
+            cur = [np.zeros_like(c) for c in cur]
 
     weight = 1.0
     scb[0] = 1
@@ -478,8 +479,7 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
                 if R_ct == 0:
                     weight = dt_dzp * dzp / total_weight
                     if want_grids:
-                        cur_s = (cur_s * weight).astype(f32)
-                        cur_x = (cur_x * weight).astype(f32)
+                        cur = [(c * weight).astype(f32) for c in cur]
                 else:
                     if ZZ[snapshot - scb[R_ct]] > sh.zpp_edge[R_ct - 1]:
                         weight = -cm.dtdz(0.5 * (ZZ[snapshot - scb[R_ct]] + sh.zpp_edge[R_ct - 1]))
@@ -507,7 +507,7 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
                     weight = 1
                     load(scb[R_ct] - 1, weight, 1)
         if want_grids:
-            grids.append((cur_s, cur_x))
+            grids.append(tuple(cur))
         R *= R_factor
     sh.final_weight = weight
     sh.zpp = np.zeros(nS)
@@ -527,7 +527,10 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
 # ---------------------------------------------------------------------------
 # frequency tables and Lyman-n sums (ComputeTs.c:760-1011)
 
-def freq_tables(p: ro.Params, T: TsTables, sh, zp, x_e_ave, collapse_fraction, ZZ, stored_fcoll, snapshot):
+def freq_tables(p: ro.Params, T: TsTables, sh, zp, x_e_ave, collapse_fraction, ZZ, stored_fcoll, snapshot,
+                agn_bands=()):
+    """Galaxy X-ray tables heat, ion, lya [14][nS], the Lyman-n sums, and for each AGN band b in
+    ``agn_bands`` (0 soft, 1 hard) its tables (ComputeTs.c:834-897) in the returned dict."""
     cm = Cosmo(p)
     nS = len(sh.R)
     ion_eff = p.ReionEfficiency
@@ -569,9 +572,9 @@ def freq_tables(p: ro.Params, T: TsTables, sh, zp, x_e_ave, collapse_fraction, Z
         r, _ = brent(lambda nu: tauX(nu, x_e, zpv, zpp) - 1, HeI_NUIONIZATION, 1e6 * NU_over_EV, 0, 0.02, 100)
         return r
 
-    thresh, alpha = p.NuXrayThreshold, p.SpecIndexXrayGal
+    thresh = p.NuXrayThreshold
 
-    def integrate_over_nu(local_x_e, lo, hi, flag):
+    def integrate_over_nu(local_x_e, lo, hi, flag, alpha=p.SpecIndexXrayGal):
         if lo >= hi:
             return 0.0
         xf = f32(local_x_e)
@@ -600,6 +603,7 @@ def freq_tables(p: ro.Params, T: TsTables, sh, zp, x_e_ave, collapse_fraction, Z
             return res * SPEED_OF_LIGHT / (4 * math.pi) / NU_LA / cm.hubble(zp)
         return res
 
+    agn = {b: [np.zeros((nx, nS)) for _ in range(3)] for b in agn_bands}
     sum_lyn = np.zeros(nS)
     first_radii, first_zero = True, True
     weight = sh.final_weight
@@ -616,6 +620,14 @@ def freq_tables(p: ro.Params, T: TsTables, sh, zp, x_e_ave, collapse_fraction, Z
             heat[k, R_ct] = integrate_over_nu(xe, lower, upper, 0)
             ion[k, R_ct] = integrate_over_nu(xe, lower, upper, 1)
             lya[k, R_ct] = integrate_over_nu(xe, lower, upper, 2)
+        zf = (1.0 + zp) / (1.0 + zpp)
+        for b in agn_bands:
+            lo_b = max(ntone, (p.NuXraySoftCut if b else thresh) * NU_over_EV * zf)
+            hi_b = (p.NuXrayMax if b else p.NuXraySoftCut) * NU_over_EV * zf
+            a_b = p.SpecIndexXrayAGNHard if b else p.SpecIndexXrayAGNSoft
+            for k in range(nx):
+                for kind in range(3):
+                    agn[b][kind][k, R_ct] = integrate_over_nu(float(T.X[k]), lo_b, hi_b, kind, a_b)
         for n_ct in range(NSPEC_MAX, 1, -1):
             if zpp > zmax(zp, n_ct):
                 continue
@@ -633,6 +645,8 @@ def freq_tables(p: ro.Params, T: TsTables, sh, zp, x_e_ave, collapse_fraction, Z
                     weight = float(f32(f32(ii) / f32(n_pts_radii)))
             sum_lyn[R_ct] = weight * sum_lyn[R_ct - 1]
             first_radii = False
+    if agn_bands:
+        return heat, ion, lya, sum_lyn, agn
     return heat, ion, lya, sum_lyn
 
 
@@ -649,7 +663,21 @@ def prefactors(p: ro.Params, zp: float):
         L *= (p.NuXrayThreshold * NU_over_EV) ** (-p.SpecIndexXrayGal) * (1 - p.SpecIndexXrayGal)
     L *= 1.0 / PLANCK
     const_zp = L / (p.NuXrayThreshold * NU_over_EV) * SPEED_OF_LIGHT * (1 + zp) ** (p.SpecIndexXrayGal + 3)
-    return dict(growth=cm.dicke(zp), dgrowth=cm.ddicke_dz(zp), dt_dzp=cm.dtdz(zp), const_zp=const_zp)
+    # AGN bands (ComputeTs.c:1049-1081,1116-1131): soft NuXrayThreshold..NuXraySoftCut, hard
+    # NuXraySoftCut..NuXrayMax, both normalised at NuXrayThreshold
+    const_agn = []
+    for b in (0, 1):
+        a = p.SpecIndexXrayAGNHard if b else p.SpecIndexXrayAGNSoft
+        lo, hi = (p.NuXraySoftCut, p.NuXrayMax) if b else (p.NuXrayThreshold, p.NuXraySoftCut)
+        if abs(a - 1.0) < float(ro.REL_TOL):
+            La = 1.0 / ((p.NuXrayThreshold * NU_over_EV) * math.log(hi / lo))
+        else:
+            La = 1.0 / ((hi * NU_over_EV) ** (1.0 - a) - (lo * NU_over_EV) ** (1.0 - a))
+            La *= (p.NuXrayThreshold * NU_over_EV) ** (-a) * (1.0 - a)
+        La /= PLANCK
+        const_agn.append(La / (p.NuXrayThreshold * NU_over_EV) * SPEED_OF_LIGHT * (1.0 + zp) ** (a + 3.0))
+    return dict(growth=cm.dicke(zp), dgrowth=cm.ddicke_dz(zp), dt_dzp=cm.dtdz(zp), const_zp=const_zp,
+                const_agn=const_agn)
 
 
 # ---------------------------------------------------------------------------
@@ -750,23 +778,39 @@ def compute_ts(p: ro.Params, T: TsTables, ZZ, snapshot: int, stored_fcoll, g: di
     xprev = g["x_e_box_prev"].astype(f32)
     x_e_ave = float(np.sum(xprev.astype(np.float64)) / n3)
     out.update(homogeneous=0, x_e_ave=x_e_ave)
+    # AGN X-ray bands in use (Flag_IncludeAGNXray 1 soft + hard, 2 hard, 3 soft)
+    bands = [b for b, on in ((0, p.Flag_IncludeAGNXray in (1, 3)), (1, p.Flag_IncludeAGNXray in (1, 2))) if on]
+    names = ("soft", "hard")
+    extra = [(g["bh_xray_" + names[b]], g.get("bh_xray_histories_" + names[b], [])) for b in bands]
     sh, grids = shells_and_sources(p, ZZ, snapshot, g["sfr"], g["xray_luminosity"], g.get("sfr_histories", []),
-                                   g.get("xray_luminosity_histories", []))
+                                   g.get("xray_luminosity_histories", []), extra=extra)
     nS = len(sh.R)
     no_light = not (collapse_fraction > 0.0)
     prevz = zp if snapshot == 0 else float(ZZ[snapshot - 1])
     dzp = zp - prevz
     pf = prefactors(p, zp)
     sums = [np.zeros(deltax.shape) for _ in range(4)]
+    sums_agn = {b: [np.zeros(deltax.shape) for _ in range(3)] for b in bands}
     if not no_light:
         sf = stored_fcoll if stored_fcoll is not None else np.zeros(len(ZZ))
-        heat, ion, lya, sum_lyn = freq_tables(p, T, sh, zp, x_e_ave, collapse_fraction, ZZ, sf, snapshot)
+        ft = freq_tables(p, T, sh, zp, x_e_ave, collapse_fraction, ZZ, sf, snapshot, agn_bands=tuple(bands))
+        heat, ion, lya, sum_lyn = ft[:4]
+        agn_tabs = ft[4] if bands else {}
         if tables_out is not None:
-            tables_out.update(heat=heat, ion=ion, lya=lya, sum_lyn=sum_lyn, shells=sh)
+            tables_out.update(heat=heat, ion=ion, lya=lya, sum_lyn=sum_lyn, shells=sh, agn=agn_tabs)
         xi = xe_interp_index(T, xprev)
         for r in range(nS):
-            shell_accumulate(p, sh, r, grids[r][0], grids[r][1], xi, (heat, ion, lya), sum_lyn, zp, sums, precision)
-        finish_sums(p, cm, pf, zp, deltax, sums)
+            agn = [(b, grids[r][2 + j], agn_tabs[b], sums_agn[b]) for j, b in enumerate(bands)]
+            shell_accumulate(p, sh, r, grids[r][0], grids[r][1], xi, (heat, ion, lya), sum_lyn, zp, sums, precision,
+                             agn=agn)
+        finish_sums(p, cm, pf, zp, deltax, sums, sums_agn)
+    # the AGN heating terms of dT_K/dz (XRayHeatingFunctions.c:1519-1520), averaged
+    xd = xprev.astype(np.float64)
+    for b in (0, 1):
+        v = 0.0
+        if b in sums_agn and not no_light:
+            v = float(np.sum(sums_agn[b][0] * pf["dt_dzp"] * 2.0 / 3.0 / BOLTZMANN / (1.0 + xd)) / n3)
+        out["volume_ave_Xheat_AGN_" + names[b]] = v
     res = evolve_cells(p, cm, T, pf, zp, dzp, deltax, xprev, g["Tk_box"], sums)
     xn, tk, ts = res["x_e"], res["Tk"], res["TS"]
     g["x_e_box_prev"][...] = xn
@@ -797,10 +841,12 @@ def xe_interp_index(T: TsTables, xprev):
 
 
 def shell_accumulate(p: ro.Params, sh, r: int, s_grid, x_grid, xi: dict, tabs, sum_lyn, zp: float, sums: list,
-                     precision: str = "fp64"):
+                     precision: str = "fp64", agn=()):
     """One shell R_ct: FFT, filter (R_ct > 0), inverse, clamp and unit conversion of the sfr and
     X-ray grids (ComputeTs.c:480-744), then its terms of the evolveInt sums
-    (XRayHeatingFunctions.c:1379-1432) added to sums = [heat, ion, lya, star]."""
+    (XRayHeatingFunctions.c:1379-1432) added to sums = [heat, ion, lya, star].  ``agn`` holds
+    (band, grid, tables, band sums) for the AGN X-ray bands: the grid clamped at 0 and converted
+    (ComputeTs.c:615-630), its terms (XRayHeatingFunctions.c:1420-1432) added to the band sums."""
     n = p.ReionGridDim
     box = p.BoxSize / p.Hubble_h
     pv = (box / float(n)) ** 3
@@ -832,15 +878,35 @@ def shell_accumulate(p: ro.Params, sh, r: int, s_grid, x_grid, xi: dict, tabs, s
     for k in range(3):
         sums[k] += dt_dzpp * dzpp * integ * fi(tabs[k])
     sums[3] += SFR * float(f32(1) + f32(zp)) ** 2 * (1 + zpp) * sum_lyn[r] * dt_dzpp * dzpp
+    for b, grid, tabs_b, sa in agn:
+        sp = ro.forward(grid, prec)
+        if r > 0:
+            sp = sp * ro.window(n, p.BoxSize, float(f32(sh.R[r])), p.TsHeatingFilterType, prec)
+        a_f = ro.inverse(sp, n)
+        if precision == "fp32":
+            a_f = a_f.astype(f32)
+        a_f = np.maximum(a_f, 0.0)
+        XA = a_f.astype(np.float64) * 1e10 * SOLAR_LUM / pv * p.UnitLength_in_cm ** -3.0
+        ia = XA * (1 + zpp) ** (-(p.SpecIndexXrayAGNHard if b else p.SpecIndexXrayAGNSoft))
+        for k in range(3):
+            sa[k] += dt_dzpp * dzpp * ia * fi(tabs_b[k])
 
 
-def finish_sums(p: ro.Params, cm: Cosmo, pf: dict, zp: float, deltax, sums: list):
-    """The prefactors evolveInt applies after its shell loop (XRayHeatingFunctions.c:1436-1447)."""
+def finish_sums(p: ro.Params, cm: Cosmo, pf: dict, zp: float, deltax, sums: list, sums_agn: dict | None = None):
+    """The prefactors evolveInt applies after its shell loop (XRayHeatingFunctions.c:1436-1470);
+    the AGN bands' terms join the heat, ion and lya sums (:1484-1540)."""
     n_b = cm.N_b0 * float(f32(1) + f32(zp)) ** 3 * (f32(1) + np.asarray(deltax, f32)).astype(np.float64)
     sums[0] *= pf["const_zp"]
     sums[1] *= pf["const_zp"]
     sums[2] *= pf["const_zp"] * n_b
     sums[3] *= (SPEED_OF_LIGHT / (4.0 * math.pi)) / (PROTONMASS / SOLAR_MASS)
+    for b, sa in (sums_agn or {}).items():
+        c = pf["const_agn"][b]
+        sa[0] *= c
+        sa[1] *= c
+        sa[2] *= c * n_b
+        for k in range(3):
+            sums[k] += sa[k]
 
 
 def evolve_cells(p: ro.Params, cm: Cosmo, T: TsTables, pf: dict, zp: float, dzp: float, deltax, xprev, Tk_box,

@@ -68,7 +68,8 @@ def test_find_hii_rejections_leave_context_usable():
 
 
 def test_compute_ts_rejections():
-    for n, kw, code in ((48, {}, rg.RG_EUNSUPPORTED), (16, {"Flag_IncludeAGNXray": 1}, rg.RG_EUNSUPPORTED),
+    for n, kw, code in ((48, {}, rg.RG_EUNSUPPORTED), (16, {"Flag_IncludeAGNXray": 1}, rg.RG_EINVAL),   # no AGN grids
+                        (16, {"Flag_IncludeAGNXray": 4}, rg.RG_EINVAL),
                         (16, {"TsNumFilterSteps": 0}, rg.RG_EINVAL), (16, {"TsHeatingFilterType": 5}, rg.RG_EINVAL)):
         dg = DeviceGrids(n, spin=True)
         p = rg.make_params(n, 32.0, Flag_IncludeSpinTemp=1, **kw)

@@ -159,8 +159,8 @@ def test_compute_ts_invalid_arguments():
     dg = DeviceGrids(n, spin=True)
     out = rg.rg_ts_scalars()
     lib = rg.load()
-    p = rg.make_params(n, 64.0, Flag_IncludeSpinTemp=1, Flag_IncludeAGNXray=1)
-    assert lib.rg_compute_Ts(ctx.h, C.byref(p), C.byref(snap), C.byref(dg.g), C.byref(out)) == rg.RG_EUNSUPPORTED
+    p = rg.make_params(n, 64.0, Flag_IncludeSpinTemp=1, Flag_IncludeAGNXray=5)
+    assert lib.rg_compute_Ts(ctx.h, C.byref(p), C.byref(snap), C.byref(dg.g), C.byref(out)) == rg.RG_EINVAL
     p = rg.make_params(n, 64.0, Flag_IncludeSpinTemp=1, TsHeatingFilterType=3)
     assert lib.rg_compute_Ts(ctx.h, C.byref(p), C.byref(snap), C.byref(dg.g), C.byref(out)) == rg.RG_EINVAL
     # shells reaching past the history slots provided
