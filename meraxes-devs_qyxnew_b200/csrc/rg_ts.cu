@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -484,9 +485,13 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
       const bool two = r + 1 < zv.nS;
       const int* src = reinterpret_cast<const int*>(gco + r);
       int* dst = reinterpret_cast<int*>(sc);
-      const int nwords = (two ? 2 : 1) * (int)(sizeof(TsShellCoef) / sizeof(int));
-      for (int i = threadIdx.x; i < (int)(2 * sizeof(TsShellCoef) / sizeof(int)); i += Z::NTH)
-        dst[i] = i < nwords ? src[i] : 0;
+      // words per shell: the AGN tables only when there are AGN units
+      constexpr int SW = (int)(sizeof(TsShellCoef) / sizeof(int));
+      constexpr int W = G > 2 ? SW : (int)(offsetof(TsShellCoef, PA) / sizeof(int));
+      for (int i = threadIdx.x; i < 2 * W; i += Z::NTH) {
+        const int sh = i / W, w = sh * SW + i % W;
+        dst[w] = (sh == 0 || two) ? src[w] : 0;
+      }
     }
     if (u + 1 < nunits)
       ts_tile_issue<N, Q>(tiles + ((u + 1) & 1) * Z::tile_elems(), unit_src(u + 1, 0), unit_src(u + 1, 1), x, y0,
