@@ -359,8 +359,9 @@ struct TsZ {
   static constexpr int NTH = T * Q;
   static constexpr int MINB = NTH >= 512 ? 1 : 512 / NTH;   // 2 blocks of 256: at most 128 registers
   static constexpr size_t tile_elems() { return (size_t)2 * (N / 2 + 1) * Q; }   // two shells' rows
+  static constexpr int STAGES = 3;           // tiles in flight: units u + 1 and u + 2 load during u
   static constexpr size_t smem() {
-    return sizeof(cf) * (N + (size_t)line_buf_r0<N, R0, Q>() + 2 * tile_elems());
+    return sizeof(cf) * (N + (size_t)line_buf_r0<N, R0, Q>() + STAGES * tile_elems());
   }
 };
 
@@ -450,16 +451,20 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
 #pragma unroll
   for (int sl = 0; sl < (G > 3 ? V : 1); ++sl) a_agn1[sl] = 0.f;
   auto addr = [&](int p) { return line_addr_r0<Z::R0, Q>(p, threadIdx.x % Q); };
-  // units u = G (r / 2) + g: the pair of shells (r, r + 1), grid g; the tile of unit u + 1 is
-  // copied while unit u is transformed
+  // units u = G (r / 2) + g: the pair of shells (r, r + 1), grid g; the tiles of units u + 1 and
+  // u + 2 are copied while unit u is transformed (three buffers)
+  constexpr int S = Z::STAGES;
   const int y0 = blockIdx.x * Q, q = threadIdx.x % Q;
   auto unit_src = [&](int u, int which) -> const cf* {
     const int r = 2 * (u / G) + which, g = u % G;
     return r < zv.nS ? work + ((size_t)r * G + g) * stride : nullptr;
   };
   const int nunits = G * ((zv.nS + 1) / 2);
-  if (nunits > 0) ts_tile_issue<N, Q>(tiles, unit_src(0, 0), unit_src(0, 1), x, y0, Z::NTH);
-  cp_async_commit();
+#pragma unroll
+  for (int u = 0; u < S - 1; ++u) {
+    if (u < nunits) ts_tile_issue<N, Q>(tiles + u * Z::tile_elems(), unit_src(u, 0), unit_src(u, 1), x, y0, Z::NTH);
+    cp_async_commit();
+  }
   // an AGN unit j: clamped at 0 (ComputeTs.c:615-630), its own band tables
   auto agn_unit = [&](const cf* tile, int j, float (&ah)[G > 2 ? V : 1]) {
     line_fft_p<PL, true>(
@@ -493,13 +498,14 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
         dst[w] = (sh == 0 || two) ? src[w] : 0;
       }
     }
-    if (u + 1 < nunits)
-      ts_tile_issue<N, Q>(tiles + ((u + 1) & 1) * Z::tile_elems(), unit_src(u + 1, 0), unit_src(u + 1, 1), x, y0,
-                          Z::NTH);
+    // buffer (u + 2) % 3 was consumed by unit u - 1 (the barrier at the end of its iteration)
+    if (u + S - 1 < nunits)
+      ts_tile_issue<N, Q>(tiles + ((u + S - 1) % S) * Z::tile_elems(), unit_src(u + S - 1, 0),
+                          unit_src(u + S - 1, 1), x, y0, Z::NTH);
     cp_async_commit();
-    cp_async_wait<1>();
+    cp_async_wait<S - 1>();   // every group but the last S - 1: unit u's tile has landed
     __syncthreads();  // unit u's tile (and the pair's coefficients) are visible to every thread
-    const cf* tile = tiles + (u & 1) * Z::tile_elems();
+    const cf* tile = tiles + (u % S) * Z::tile_elems();
     if (g == 0) {
       // sfr: stellar Lyman-alpha sum, SFR clamped at 0 (ComputeTs.c:700)
       const float c0 = sc[0].cstar, c1 = sc[1].cstar;
@@ -524,7 +530,7 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
         agn_unit(tile, 1, a_agn1);
       }
     }
-    __syncthreads();  // the tile is consumed before unit u + 2 refills it
+    __syncthreads();  // the tile is consumed before unit u + 3 refills it
   }
 #pragma unroll
   for (int sl = 0; sl < V; ++sl) {
