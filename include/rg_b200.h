@@ -78,6 +78,14 @@ typedef struct rg_params {
      nu^-alpha indices of the soft (NuXrayThreshold..NuXraySoftCut) and hard
      (NuXraySoftCut..NuXrayMax) bands (meraxes.h:187-189) */
   double SpecIndexXrayAGNSoft, SpecIndexXrayAGNHard;
+  /* Pop III sources in find_HII_bubbles, as a USE_MINI_HALOS build of the reference has them
+     (find_HII_bubbles.c:104-117,190-202,443-450,460-545): 1 = starsIII and weighted_sfrIII enter
+     the barrier, J_21 and Gamma12 with their own efficiency and photons per baryon (the caller
+     sets ReionNionPhotPerBaryIII from its Pop III IMF, PopIII.c:94, and ReionEfficiencyIII as
+     set_ReionEfficiency does).  The Pop III channels of ComputeTs and delta_T are not built:
+     rg_compute_Ts and rg_delta_T return RG_EUNSUPPORTED with UseMiniHalos. */
+  int UseMiniHalos;
+  double ReionEfficiencyIII, ReionNionPhotPerBaryIII;
 } rg_params;
 
 /* Fill *p with the values of input/params/defaults.par and the Genesis cosmology/units. */
@@ -133,6 +141,9 @@ typedef struct rg_grids {
   const float* bh_xray_hard;
   const float* bh_xray_histories_soft;
   const float* bh_xray_histories_hard;
+  /* Pop III stellar mass and escape-weighted SFR (UseMiniHalos), padded */
+  const float* starsIII;
+  const float* weighted_sfrIII;
 } rg_grids;
 
 /* The snapshot being processed: run_globals.ZZ[] and the snapshot index into it. */
@@ -160,6 +171,7 @@ typedef struct rg_hii_scalars {
   double volume_weighted_global_residual_xH, volume_weighted_global_clumping_factor;
   double mass_weighted_global_Gamma12, mass_weighted_global_N_rec;
   double mass_weighted_global_residual_xH, mass_weighted_global_clumping_factor;
+  double volume_weighted_global_weighted_sfrIII;   /* UseMiniHalos only (0 otherwise) */
 } rg_hii_scalars;
 
 typedef struct rg_ts_scalars {

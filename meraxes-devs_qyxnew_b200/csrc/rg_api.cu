@@ -271,6 +271,11 @@ int rg_params_default(rg_params* p, int grid_dim, double box_size) {
   p->Flag_TemperatureDependentRec = 1;   // input/params/defaults.par:19
   p->SpecIndexXrayAGNSoft = 2.2;          // input/params/defaults.par:67-68
   p->SpecIndexXrayAGNHard = 1.7;
+  // Pop III (UseMiniHalos): the caller's IMF sets the photons per baryon; the efficiency follows
+  // set_ReionEfficiency (reionization.c:311-314)
+  p->UseMiniHalos = 0;
+  p->ReionNionPhotPerBaryIII = p->ReionNionPhotPerBary;
+  p->ReionEfficiencyIII = 1.0 / p->BaryonFrac * p->ReionNionPhotPerBaryIII / (1.0 - 0.75 * p->Y_He);
   return RG_OK;
 }
 
@@ -415,6 +420,10 @@ int rg_alloc_grids(rg_context* ctx, const rg_params* p, int n_hist, rg_grids* ou
   RG_ALLOC(temp_kinetic_all_gas, nreal);
   RG_ALLOC(delta_T, nreal);
   if (p->Flag_IncludeSpinTemp && p->Flag_IncludePecVelsFor21cm > 0) RG_ALLOC(vel, npad);
+  if (p->UseMiniHalos) {
+    RG_ALLOC(starsIII, npad);
+    RG_ALLOC(weighted_sfrIII, npad);
+  }
   if (p->Flag_IncludeRecombinations) {
     RG_ALLOC(Gamma12, nreal);
     RG_ALLOC(N_rec, npad);
@@ -492,6 +501,8 @@ static int find_hii(rg_context* ctx, const rg_params* p, const rg_snapshot* s, c
     return set_error(ctx, RG_EINVAL, "spin temperature needs x_e_box and Tk_box");
   if (p->Flag_BHFeedback && (!g->effective_bhm || !g->effective_bhar))
     return set_error(ctx, RG_EINVAL, "BH feedback needs effective_bhm and effective_bhar");
+  if (p->UseMiniHalos && (!g->starsIII || !g->weighted_sfrIII))
+    return set_error(ctx, RG_EINVAL, "UseMiniHalos needs starsIII and weighted_sfrIII");
   if ((rc = ensure_tables(ctx, p))) return rc;
   cudaSetDevice(ctx->device);
   return hii_snapshot(ctx, p, s, g, out, stg);
@@ -593,11 +604,13 @@ static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
   const bool need_spin = p->Flag_IncludeSpinTemp != 0;
   const bool need_bh = p->Flag_BHFeedback != 0;
   const bool need_rec = p->Flag_IncludeRecombinations != 0;
+  const bool need_mini = p->UseMiniHalos != 0;
   if (ctx->dev_grids_ready) {
     const bool has_spin = ctx->dev_grids.Tk_box != nullptr;
     const bool has_bh = ctx->dev_grids.effective_bhm != nullptr;
     const bool has_rec = ctx->dev_grids.Gamma12 != nullptr;
-    if ((!need_spin || has_spin) && (!need_bh || has_bh) && (!need_rec || has_rec) &&
+    const bool has_mini = ctx->dev_grids.starsIII != nullptr;
+    if ((!need_spin || has_spin) && (!need_bh || has_bh) && (!need_rec || has_rec) && (!need_mini || has_mini) &&
         ctx->dev_grids_nhist >= n_hist)
       return RG_OK;
     for (void* q : ctx->owned) cudaFree(q);
@@ -615,10 +628,17 @@ static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
 // transformed (they go with the first group of uploads); r_bubble and the recombination grids
 // come back after the step.
 static int hii_rec_inputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t cs) {
-  if (!p->Flag_IncludeRecombinations) return RG_OK;
   const rg_grids& d = ctx->dev_grids;
   const size_t n = (size_t)ctx->N;
   const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float);
+  if (p->UseMiniHalos) {
+    // Pop III grids: both transformed with recombinations, weighted_sfrIII otherwise only summed
+    if (!h->starsIII || !h->weighted_sfrIII) return set_error(ctx, RG_EINVAL, "UseMiniHalos needs starsIII and weighted_sfrIII");
+    int r = copy_grid(ctx, (void*)d.starsIII, h->starsIII, bp, cudaMemcpyHostToDevice, cs);
+    if (!r) r = copy_grid(ctx, (void*)d.weighted_sfrIII, h->weighted_sfrIII, bp, cudaMemcpyHostToDevice, cs);
+    if (r) return r;
+  }
+  if (!p->Flag_IncludeRecombinations) return RG_OK;
   if (!h->N_rec || !h->Gamma12 || !h->residual_xH || !h->clumping_factor || !h->t_resp)
     return set_error(ctx, RG_EINVAL, "recombinations need Gamma12, N_rec, residual_xH, clumping_factor, t_resp");
   int rc = copy_grid(ctx, d.N_rec, h->N_rec, bp, cudaMemcpyHostToDevice, cs);
@@ -771,6 +791,8 @@ static int compute_ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s,
     return set_error(ctx, RG_EUNSUPPORTED, "ComputeTs needs a power-of-two ReionGridDim");
   if (p->Flag_IncludeAGNXray < 0 || p->Flag_IncludeAGNXray > 3)
     return set_error(ctx, RG_EINVAL, "Flag_IncludeAGNXray must be 0, 1, 2 or 3");
+  if (p->UseMiniHalos)
+    return set_error(ctx, RG_EUNSUPPORTED, "UseMiniHalos: the Pop III channels of ComputeTs are not built");
   if (p->TsHeatingFilterType < 0 || p->TsHeatingFilterType > 2)
     return set_error(ctx, RG_EINVAL, "TsHeatingFilterType must be 0, 1 or 2");
   if (p->TsNumFilterSteps < 1 || p->TsNumFilterSteps > 1024)

@@ -287,6 +287,8 @@ int rg_delta_T(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const 
   if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return set_error(ctx, RG_EINVAL, "snapshot out of range");
   if (p->Flag_IncludePecVelsFor21cm < 0 || p->Flag_IncludePecVelsFor21cm > 3)
     return set_error(ctx, RG_EINVAL, "Flag_IncludePecVelsFor21cm must be 0, 1, 2 or 3");
+  if (p->UseMiniHalos)
+    return set_error(ctx, RG_EUNSUPPORTED, "UseMiniHalos: the Pop II brightness temperature delta_TII is not built");
   const bool vel_modes = p->Flag_IncludeSpinTemp && p->Flag_IncludePecVelsFor21cm > 0;
   if (!g->xH || !g->deltax || !g->delta_T || (p->Flag_IncludeSpinTemp && !g->TS_box) || (vel_modes && !g->vel))
     return set_error(ctx, RG_EINVAL, "missing grid pointer");

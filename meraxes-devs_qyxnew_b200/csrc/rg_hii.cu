@@ -182,6 +182,8 @@ struct HiiBatch {
   double fcoll_pref[KB_MAX];
   float J_aux[KB_MAX], J_aux_bh[KB_MAX];
   float G_pref[KB_MAX], G_pref_bh[KB_MAX], R[KB_MAX];   // recombination branch
+  double fcoll_prefIII[KB_MAX];                          // Pop III (mini-halos)
+  float J_auxIII[KB_MAX], G_prefIII[KB_MAX];
 };
 
 struct HiiState {
@@ -193,6 +195,7 @@ struct HiiState {
   const float* deltax_unf;   // padded
   const float* wsfr;         // padded
   const float* bhar;         // padded, may be null
+  const float* wsfrIII;      // padded, Pop III only
   float* Gamma12;            // recombination branch: written at a cell's first crossing
   float* r_bubble;
   uint32_t* bits;            // [2][nblocks][W][NTH]
@@ -220,9 +223,10 @@ struct HiiZ {
 
 // z pass of a batch.  FINAL: the batch ends with the snapshot's last (unfiltered) radius.
 // Grids in rt: 0 deltax, 1 stars, then x_e (spin temperature), then effective_bhm (BH), then
-// with recombinations N_rec, weighted_sfr and effective_bhar (BH).  NG is the number of grids,
-// or 7 for any count from 4 to 7 (then bt.ng), which is the one used with recombinations.
-template <int N, int NG, bool FINAL>
+// starsIII (Pop III), then with recombinations N_rec, weighted_sfr, effective_bhar (BH) and
+// weighted_sfrIII (Pop III).  NG is the number of grids; the EXT instantiation (recombinations or
+// Pop III) takes any count up to NG from bt.ng.
+template <int N, int NG, bool FINAL, bool EXT>
 __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
     k_hii_z(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
             HiiState s) {
@@ -265,15 +269,18 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
       I[w] = s.bits[nwords + (blk * W + w) * NTH + threadIdx.x];
     }
   }
-  const int ng = NG == 7 ? bt.ng : NG;
-  const int gx = c.spin ? 2 : -1;
-  const int gb = c.bh ? (c.spin ? 3 : 2) : -1;
-  // the recombination grids (only the 7-grid instantiation runs with recombinations, so the
-  // others compile without this branch)
-  const bool rec = NG == 7 && c.rec;
-  const int gn = rec ? 2 + c.spin + c.bh : -1;     // N_rec
-  const int gw = rec ? gn + 1 : -1;                // weighted_sfr
-  const int gr = rec && c.bh ? gn + 2 : -1;        // effective_bhar
+  // the Pop III and recombination grids (only the 9-grid instantiation runs with them, so the
+  // others compile without those branches)
+  const int ng = EXT ? bt.ng : NG;
+  const bool rec = EXT && c.rec, mini = EXT && c.mini;
+  int gi = 2;
+  const int gx = c.spin ? gi++ : -1;
+  const int gb = c.bh ? gi++ : -1;
+  const int gm = mini ? gi++ : -1;                 // starsIII
+  const int gn = rec ? gi++ : -1;                  // N_rec
+  const int gw = rec ? gi++ : -1;                  // weighted_sfr
+  const int gr = rec && c.bh ? gi++ : -1;          // effective_bhar
+  const int gw3 = rec && mini ? gi++ : -1;         // weighted_sfrIII
   double acc[FINAL ? HII_NSUM : 1];
 #pragma unroll
   for (int k = 0; k < (FINAL ? HII_NSUM : 1); ++k) acc[k] = 0.0;
@@ -334,6 +341,11 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
           bhm = fmaxf(rt[(gb * ROWS + row) * RP + z], 0.f);
           if (bhm < ABS_TOL) bhm = 0.f;
         }
+        float stIII = 0.f;
+        if (gm >= 0) {
+          stIII = fmaxf(rt[(gm * ROWS + row) * RP + z], 0.f);
+          if (stIII < ABS_TOL) stIII = 0.f;
+        }
         float nrec = 0.f;
         if (gn >= 0) {
           nrec = fmaxf(rt[(gn * ROWS + row) * RP + z], 0.f);
@@ -345,7 +357,9 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
         // (f_bh + f_stars) * prefactor > nf (1 + rec) with f = grid / dom, tested with both
         // sides times dom: the two forms differ only within a few FP64 ulps of the barrier
         const double num = c.bh ? (double)bhm + (double)st : (double)st;
-        const bool ion = num * pref > nf * (1.0 + rec) * dom;
+        const double prefIII = gm >= 0 ? bt.fcoll_prefIII[r] : 0.0;
+        const double lhs_dom = gm >= 0 ? num * pref + (double)stIII * prefIII : num * pref;
+        const bool ion = lhs_dom > nf * (1.0 + rec) * dom;
         float xH = (iw & bit) ? 0.f : 1.f;   // so far: 0 once ionized at a radius, else 1
         const size_t cellrow = (size_t)x * N + y0 + row;
         const size_t ir = cellrow * N + z;
@@ -356,6 +370,11 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
             float wsf = fmaxf(rt[(gw * ROWS + row) * RP + z], 0.f);
             if (wsf < ABS_TOL) wsf = 0.f;
             float G = __fmul_rn(wsf, bt.G_pref[r]);
+            if (gw3 >= 0) {
+              float w3 = fmaxf(rt[(gw3 * ROWS + row) * RP + z], 0.f);
+              if (w3 < ABS_TOL) w3 = 0.f;
+              G = __fadd_rn(G, __fmul_rn(w3, bt.G_prefIII[r]));
+            }
             if (gr >= 0) {
               float bhr = fmaxf(rt[(gr * ROWS + row) * RP + z], 0.f);
               if (bhr < ABS_TOL) bhr = 0.f;
@@ -365,6 +384,7 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
             s.r_bubble[ir] = bt.R[r];
             if (c.uvb == 2) {
               float j = __fmul_rn(st, bt.J_aux[r]);
+              if (gm >= 0) j = __fadd_rn(j, __fmul_rn(stIII, bt.J_auxIII[r]));
               if (c.bh) j = __fadd_rn(j, __fmul_rn(bhm, bt.J_aux_bh[r]));
               s.J21[ir] = j;
             }
@@ -384,7 +404,8 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
           const double fcs = (double)st / dom;
           const double fbh = c.bh ? (double)bhm / dom : 0.0;
           const double lhs = (fbh + fcs) * pref;
-          const float v = (float)(nf - lhs);
+          float v = (float)(nf - lhs);
+          if (gm >= 0) v -= (float)((double)stIII / dom * prefIII);   // a float subtraction in the C
           xH = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
         }
         float zin_new = -1.f;                // > -1: set this radius
@@ -395,6 +416,7 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
           s.z_in[ir] = zin_new;
           if (c.uvb == 1) {
             float j = st * bt.J_aux[r];
+            if (gm >= 0) j = __fadd_rn(j, __fmul_rn(stIII, bt.J_auxIII[r]));
             if (c.bh) j += bhm * bt.J_aux_bh[r];
             s.J21[ir] = j;
           }
@@ -423,6 +445,7 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
           // (find_HII_bubbles.c:490-508); its sums come from k_hii_recomb.
           acc[2] += (double)s.wsfr[ip];
           if (s.bhar != nullptr) acc[3] += (double)s.bhar[ip];
+          if (s.wsfrIII != nullptr) acc[9] += (double)s.wsfrIII[ip];
           acc[4] += (double)temp;
           acc[5] += (double)xH * domu;
           acc[7] += (double)temp * domu;
@@ -680,7 +703,16 @@ int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, cf* work, size_t 
   return RG_OK;
 }
 
-template <int N, int NG, bool FINAL>
+// grids one EXT z pass can hold at this size: the most, up to 9, whose row buffers fit the
+// 227 KB of shared memory a block may use (7 at 384^3, 8 at 192^3)
+template <int N>
+constexpr int hii_ngx() {
+  int ng = 9;
+  while (ng > 4 && HiiZ<N, true>::smem(ng) > 227 * 1024) --ng;
+  return ng;
+}
+
+template <int N, int NG, bool FINAL, bool EXT = false>
 int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch& bt, const HiiConst& c,
                   const HiiState& s, cudaStream_t st, int* nblocks) {
   const cf* tw;
@@ -689,16 +721,16 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   using C = Cfg<N>;
   static_assert(HiiZ<N, FINAL>::smem(NG) <= 227 * 1024, "z pass shared memory above the per-block limit");
   const size_t sm = HiiZ<N, FINAL>::smem(NG);
-  RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL>, sm));
+  RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL, EXT>, sm));
   const dim3 grid(N / (2 * C::QZ), N);
   // algorithmic bytes: the Hermitian halves of NG grids per radius, z_at_ionization on the
   // first batch; the closing pass writes xH and temperature and reads deltax, weighted_sfr,
   // [effective_bhar], [Tk_box]
   const double n3 = (double)N * N * N, nzc = (double)C::NZ * N * N;
-  double bytes = bt.nr * (NG == 7 ? bt.ng : NG) * 8.0 * nzc + (bt.first ? 4.0 * n3 : 0.0);
+  double bytes = bt.nr * (EXT ? bt.ng : NG) * 8.0 * nzc + (bt.first ? 4.0 * n3 : 0.0);
   if (FINAL) bytes += 4.0 * n3 * (2 + 2 + (s.bhar != nullptr) + (s.Tk_box != nullptr));
   prof_begin(ctx, FINAL ? "inv_z_c2r_test_final" : "inv_z_c2r_test", st);
-  k_hii_z<N, NG, FINAL><<<grid, C::T * C::QZ, sm, st>>>(work, stride, tw, bt, c, s);
+  k_hii_z<N, NG, FINAL, EXT><<<grid, C::T * C::QZ, sm, st>>>(work, stride, tw, bt, c, s);
   prof_end(ctx, bytes, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   if (nblocks) *nblocks = (int)(grid.x * grid.y);
@@ -708,10 +740,17 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
 template <int N>
 int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
                  const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
-  // with recombinations (4 to 7 grids) one instantiation reads the count from the batch
-  if (c.rec)
-    return fin ? launch_hii_z3<N, 7, true>(ctx, work, stride, bt, c, s, st, nblocks)
-               : launch_hii_z3<N, 7, false>(ctx, work, stride, bt, c, s, st, nblocks);
+  // with recombinations or Pop III (up to 9 grids) one instantiation reads the count from the
+  // batch
+  if (c.rec || c.mini) {
+    constexpr int NGX = hii_ngx<N>();
+    if (ng > NGX)
+      return set_error(ctx, RG_EUNSUPPORTED,
+                       "this combination of grids (recombinations, Pop III, BH feedback, spin temperature) needs "
+                       "more row buffers than one z pass holds at this ReionGridDim");
+    return fin ? launch_hii_z3<N, NGX, true, true>(ctx, work, stride, bt, c, s, st, nblocks)
+               : launch_hii_z3<N, NGX, false, true>(ctx, work, stride, bt, c, s, st, nblocks);
+  }
   if (ng == 2)
     return fin ? launch_hii_z3<N, 2, true>(ctx, work, stride, bt, c, s, st, nblocks)
                : launch_hii_z3<N, 2, false>(ctx, work, stride, bt, c, s, st, nblocks);
@@ -852,6 +891,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   const int N = ctx->N;
   const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
   const bool rec = p->Flag_IncludeRecombinations != 0;
+  const bool mini = p->UseMiniHalos != 0;
   const double redshift = s->ZZ[s->snapshot];
   const double box_size = p->BoxSize;
   const double pixel_volume = std::pow(box_size / (double)N, 3);
@@ -867,21 +907,24 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   c.spin = spin;
   c.bh = bh;
   c.rec = rec;
+  c.mini = mini;
 
   // Grids to transform: the ones the z pass reads, in its order.  weighted_sfr (and
   // effective_bhar) feed only Gamma12 on the recombination branch, so without it their
   // filtered fields are never read; the plain mode transforms weighted_sfr anyway, as the
   // reference does.
-  const float* srcs[8];
+  const float* srcs[10];
   int ng = 0;
   srcs[ng++] = g->deltax;
   srcs[ng++] = g->stars;
   if (spin) srcs[ng++] = g->x_e_box;
   if (bh) srcs[ng++] = g->effective_bhm;
+  if (mini) srcs[ng++] = g->starsIII;
   if (rec) {
     srcs[ng++] = g->N_rec;
     srcs[ng++] = g->weighted_sfr;
     if (bh) srcs[ng++] = g->effective_bhar;
+    if (mini) srcs[ng++] = g->weighted_sfrIII;
   }
   const int ntest = ng;
   const bool plain = ctx->mode == RG_MODE_PLAIN;
@@ -898,7 +941,10 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   const size_t nw = bit_words(N);
   if ((rc = ensure_device(ctx, &ctx->bits, &ctx->bits_elems, 2 * nw))) return rc;
   if ((rc = stage_wait(ctx, stg->inputs, st))) return rc;
-  if ((rc = fft_forward(ctx, N, srcs, ng, ctx->spec, nc, 1.0 / std::pow((double)N, 3), st))) return rc;
+  for (int g0 = 0; g0 < ng; g0 += MAXG)   // at most MAXG grids per forward launch
+    if ((rc = fft_forward(ctx, N, srcs + g0, std::min(MAXG, ng - g0), ctx->spec + nc * g0, nc,
+                          1.0 / std::pow((double)N, 3), st)))
+      return rc;
 
   // window table for all radii
   const int n2max = 3 * (N / 2) * (N / 2);
@@ -935,6 +981,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   hs.deltax_unf = g->deltax;
   hs.wsfr = g->weighted_sfr;
   hs.bhar = bh ? g->effective_bhar : nullptr;
+  hs.wsfrIII = mini ? g->weighted_sfrIII : nullptr;
   hs.Gamma12 = g->Gamma12;
   hs.r_bubble = g->r_bubble;
   hs.bits = ctx->bits;
@@ -967,6 +1014,10 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
       bt.G_pref_bh[k] = (float)G_bh;
       bt.R[k] = (float)R;
       bt.fcoll_pref[k] = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R * R * R;
+      // Pop III (find_HII_bubbles.c:443-450): photons per baryon and efficiency of their own
+      bt.J_auxIII[k] = bt.J_aux[k] * (float)(p->ReionNionPhotPerBaryIII / p->ReionNionPhotPerBary);
+      bt.G_prefIII[k] = (float)(Gamma_R_prefactor * p->ReionNionPhotPerBaryIII / p->ReionNionPhotPerBary);
+      bt.fcoll_prefIII[k] = bt.fcoll_pref[k] / p->ReionEfficiency * p->ReionEfficiencyIII;
     }
     // the snapshot's last radius is unfiltered (find_HII_bubbles.c:313)
     const int unf = fin ? cnt - 1 : -1;
@@ -1028,6 +1079,8 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   out->mass_weighted_global_r_bubble = S[6] / mass_weight;
   out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
   out->n_radii = nr;
+  out->volume_weighted_global_weighted_sfrIII =
+      mini ? S[9] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS : 0.0;
   const double* R = S + 16;   // recombination sums (find_HII_bubbles.c:666-684)
   out->volume_weighted_global_Gamma12 = rec ? R[2] / n3 : 0.0;
   out->volume_weighted_global_N_rec = rec ? R[4] / n3 : 0.0;

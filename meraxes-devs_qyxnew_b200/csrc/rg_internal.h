@@ -93,7 +93,7 @@ int ensure_device(rg_context* ctx, T** ptr, size_t* have, size_t need) {
 // Per-snapshot constants of the barrier test.
 struct HiiConst {
   float redshift, TK, cT_ad;
-  int uvb, spin, bh, rec;
+  int uvb, spin, bh, rec, mini;
 };
 
 // Recombination tables on the device (splined_recombination, recombinations.c:35-84).
@@ -105,7 +105,7 @@ struct RecTables {
   double lng_lo, lng_hi; // knots[0] and the float-rounded upper bound of the table
 };
 
-constexpr int HII_NSUM = 9;   // closing-pass sums
+constexpr int HII_NSUM = 10;  // closing-pass sums
 constexpr int KB_MAX = 16;    // radii per batch
 
 // Forward r2c of ng padded real grids into spectra spec_base + g * stride, scaled.

@@ -43,6 +43,7 @@ class rg_params(C.Structure):
         ("TreesID", C.c_int),
         ("Flag_TemperatureDependentRec", C.c_int),
         ("SpecIndexXrayAGNSoft", C.c_double), ("SpecIndexXrayAGNHard", C.c_double),
+        ("UseMiniHalos", C.c_int), ("ReionEfficiencyIII", C.c_double), ("ReionNionPhotPerBaryIII", C.c_double),
     ]
 
 
@@ -65,6 +66,7 @@ class rg_grids(C.Structure):
         ("clumping_factor", C.c_void_p), ("t_resp", C.c_void_p),
         ("bh_xray_soft", C.c_void_p), ("bh_xray_hard", C.c_void_p), ("bh_xray_histories_soft", C.c_void_p),
         ("bh_xray_histories_hard", C.c_void_p),
+        ("starsIII", C.c_void_p), ("weighted_sfrIII", C.c_void_p),
     ]
 
 
@@ -81,7 +83,8 @@ class rg_hii_scalars(C.Structure):
         ("n_radii", C.c_int)] + [(n, C.c_double) for n in (
         "volume_weighted_global_Gamma12", "volume_weighted_global_N_rec", "volume_weighted_global_residual_xH",
         "volume_weighted_global_clumping_factor", "mass_weighted_global_Gamma12", "mass_weighted_global_N_rec",
-        "mass_weighted_global_residual_xH", "mass_weighted_global_clumping_factor")]
+        "mass_weighted_global_residual_xH", "mass_weighted_global_clumping_factor",
+        "volume_weighted_global_weighted_sfrIII")]
 
     def as_dict(self):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}

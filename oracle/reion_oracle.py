@@ -97,6 +97,9 @@ class Params:
     Flag_TemperatureDependentRec: int = 1
     SpecIndexXrayAGNSoft: float = 2.2
     SpecIndexXrayAGNHard: float = 1.7
+    UseMiniHalos: int = 0
+    ReionEfficiencyIII: float = 1.0
+    ReionNionPhotPerBaryIII: float = 4000.0
 
 
 @dataclasses.dataclass
@@ -316,7 +319,8 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
                      Tk_box: np.ndarray | None = None, effective_bhm: np.ndarray | None = None,
                      effective_bhar: np.ndarray | None = None, record_margins: bool = False,
                      radius_subset: int | None = None, with_dead_grids: bool = False, rec_tables=None,
-                     prev_z: float | None = None):
+                     prev_z: float | None = None, starsIII: np.ndarray | None = None,
+                     weighted_sfrIII: np.ndarray | None = None):
     """Restatement of _find_HII_bubbles() (find_HII_bubbles.c:86-710), one rank.
 
     With ``Flag_IncludeRecombinations`` the state carries Gamma12 and N_rec, ``rec_tables`` is a
@@ -325,6 +329,11 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     tested against 1 + N_rec (:467-483), Gamma12, r_bubble (and J_21 for ReionUVBFlag 2) are
     recorded at each cell's first crossing (:488-508), and the closing pass updates N_rec and
     returns residual_xH, clumping_factor and t_resp in ``diag["rec"]`` (:612-644).
+
+    With ``UseMiniHalos`` (a USE_MINI_HALOS build) the padded Pop III grids ``starsIII`` and
+    ``weighted_sfrIII`` add f_coll_starsIII x f_coll_prefactorIII to the barrier, to J_21 and
+    (with recombinations) to Gamma12 (:104-117,190-202,443-545), and weighted_sfrIII to the
+    closing-pass averages.
 
     Inputs are padded float32 grids; ``state`` is updated in place.  Returns
     ``(xH, r_bubble, scalars, diag)`` where ``diag`` holds, when
@@ -339,6 +348,9 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     import time as _time
     t_start = _time.perf_counter()
     rec = bool(p.Flag_IncludeRecombinations)
+    mini = bool(p.UseMiniHalos)
+    if mini and (starsIII is None or weighted_sfrIII is None):
+        raise ValueError("UseMiniHalos needs starsIII and weighted_sfrIII")
     if rec and (rec_tables is None or state.Gamma12 is None or state.N_rec is None):
         raise ValueError("recombinations need rec_tables and a state with Gamma12 and N_rec")
     n = p.ReionGridDim
@@ -362,11 +374,15 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
         grids["x_e"] = x_e_box[:, :, :n]
     if p.Flag_BHFeedback:
         grids["bhm"] = effective_bhm[:, :, :n]
+    if mini:
+        grids["starsIII"] = starsIII[:, :, :n]
     if rec:
         grids["nrec"] = state.N_rec
         grids["wsfr"] = weighted_sfr[:, :, :n]
         if p.Flag_BHFeedback:
             grids["bhar"] = effective_bhar[:, :, :n]
+        if mini:
+            grids["wsfrIII"] = weighted_sfrIII[:, :, :n]
     if with_dead_grids:
         grids["wsfr"] = weighted_sfr[:, :, :n]
     spectra = {k: forward(v, precision) for k, v in grids.items()}
@@ -427,11 +443,19 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
         fcoll_pref = p.ReionEfficiency * (4.0 / 3.0) * math.pi / pixel_volume / M_mean * R ** 3
         G_pref_bh = g_pref * (SIGMA_HI * p.ReionAlphaUVBH / (p.ReionAlphaUVBH + 2.75) * 1e12)
         G_pref = g_pref * (SIGMA_HI * p.ReionAlphaUV / (p.ReionAlphaUV + 2.75) * 1e12)
+        # Pop III (find_HII_bubbles.c:443-450)
+        J_auxIII = f32(J_aux * f32(p.ReionNionPhotPerBaryIII / p.ReionNionPhotPerBary))
+        G_prefIII = G_pref * p.ReionNionPhotPerBaryIII / p.ReionNionPhotPerBary
+        fcoll_prefIII = fcoll_pref / p.ReionEfficiency * p.ReionEfficiencyIII
 
         dom = 1.0 + fd.astype(np.float64)
         fcs = fs.astype(np.float64) / dom
         fbh = fb.astype(np.float64) / dom if fb is not None else 0.0
         lhs = (fbh + fcs) * fcoll_pref
+        lhs_II = lhs
+        fsIII = clamped("starsIII") if mini else None
+        if mini:
+            lhs = lhs + fsIII.astype(np.float64) / dom * fcoll_prefIII
         recf = clamped("nrec").astype(np.float64) / dom if rec else 0.0
         rhs = neutral * (1.0 + recf)
         ion = lhs > rhs
@@ -439,12 +463,16 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
             # first crossing of the snapshot (find_HII_bubbles.c:488-508)
             first = ion & (xH > REL_TOL)
             gam = (clamped("wsfr")[first].astype(f32) * f32(G_pref)).astype(f32)
+            if mini:
+                gam = (gam + (clamped("wsfrIII")[first].astype(f32) * f32(G_prefIII)).astype(f32)).astype(f32)
             if p.Flag_BHFeedback:
                 gam = (gam + (clamped("bhar")[first].astype(f32) * f32(G_pref_bh)).astype(f32)).astype(f32)
             state.Gamma12[first] = gam
             r_bubble[first] = f32(R)
             if p.ReionUVBFlag == 2:
                 jj = (fs[first].astype(f32) * J_aux).astype(f32)
+                if mini:
+                    jj = (jj + (fsIII[first].astype(f32) * J_auxIII).astype(f32)).astype(f32)
                 if fb is not None:
                     jj = (jj + (fb[first].astype(f32) * J_aux_bh).astype(f32)).astype(f32)
                 J21[first] = jj
@@ -461,12 +489,16 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
             else:
                 t_hi = (float(TK) * (1.0 + (cT_ad * dx_real[partial]).astype(f32).astype(np.float64))).astype(f32)
             temp[partial] = partially_ionized_temperature(t_hi, xH[partial])
-            v = (neutral[partial] - lhs[partial]).astype(f32)
+            v = (neutral[partial] - lhs_II[partial]).astype(f32)
+            if mini:
+                v = (v - (fsIII[partial].astype(np.float64) / dom[partial] * fcoll_prefIII).astype(f32)).astype(f32)
             xH[partial] = np.clip(v, 0, 1)
         new = (xH < REL_TOL) & (z_in < 0)
         z_in[new] = f32(z)
         if p.ReionUVBFlag == 1:
             jj = (fs[new].astype(f32) * J_aux).astype(f32)
+            if mini:
+                jj = (jj + (fsIII[new].astype(f32) * J_auxIII).astype(f32)).astype(f32)
             if fb is not None:
                 jj = (jj + (fb[new].astype(f32) * J_aux_bh).astype(f32)).astype(f32)
             J21[new] = jj
@@ -497,6 +529,10 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     else:
         s["volume_weighted_global_effective_bhar"] = 0.0
     s["volume_weighted_global_temp_kinetic_all_gas"] = temp.astype(np.float64).sum() / n3
+    s["volume_weighted_global_weighted_sfrIII"] = 0.0
+    if mini:
+        w3 = weighted_sfrIII[:, :, :n].astype(np.float64).sum() / n3
+        s["volume_weighted_global_weighted_sfrIII"] = w3 * p.UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS
     mw = dom.sum()
     s["mass_weighted_global_xH"] = (xH.astype(np.float64) * dom).sum() / mw
     s["mass_weighted_global_r_bubble"] = (r_bubble.astype(np.float64) * dom).sum() / mw
