@@ -624,10 +624,11 @@ static int ensure_dev_grids(rg_context* ctx, const rg_params* p, int n_hist) {
   return RG_OK;
 }
 
-// Recombination branch of the host forms: N_rec, weighted_sfr and effective_bhar are then
-// transformed (they go with the first group of uploads); r_bubble and the recombination grids
-// come back after the step.
-static int hii_rec_inputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t cs) {
+// The Pop III and recombination grids of the host forms: starsIII and weighted_sfrIII (Pop III),
+// and with recombinations N_rec and effective_bhar, go with the first group of uploads (they are
+// transformed, or with weighted_sfrIII only summed); r_bubble and the recombination grids come
+// back after the step.
+static int hii_extra_inputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t cs) {
   const rg_grids& d = ctx->dev_grids;
   const size_t n = (size_t)ctx->N;
   const size_t bp = n * n * 2 * (n / 2 + 1) * sizeof(float);
@@ -647,7 +648,7 @@ static int hii_rec_inputs(rg_context* ctx, const rg_params* p, const rg_grids* h
   return rc;
 }
 
-static int hii_rec_outputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t st) {
+static int hii_extra_outputs(rg_context* ctx, const rg_params* p, const rg_grids* h, cudaStream_t st) {
   if (!p->Flag_IncludeRecombinations) return RG_OK;
   const rg_grids& d = ctx->dev_grids;
   const size_t n = (size_t)ctx->N;
@@ -684,7 +685,7 @@ int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snaps
   if (p->Flag_IncludeSpinTemp && (rc = copy_grid(ctx, (void*)d.x_e_box, h->x_e_box, bp, H2D, cs))) return rc;
   const bool rec = p->Flag_IncludeRecombinations != 0;
   if (p->Flag_BHFeedback && (rc = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D, cs))) return rc;
-  if ((rc = hii_rec_inputs(ctx, p, h, cs))) return rc;
+  if ((rc = hii_extra_inputs(ctx, p, h, cs))) return rc;
   if ((plain || rec) && (rc = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return rc;
   if ((rc = stage_record(ctx, 1, cs, &stg.inputs))) return rc;
   if ((rc = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D, cs))) return rc;
@@ -709,7 +710,7 @@ int rg_find_HII_bubbles_host(rg_context* ctx, const rg_params* p, const rg_snaps
   if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H))) return rc;
   if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H))) return rc;
-  if ((rc = hii_rec_outputs(ctx, p, h, ctx->stream))) return rc;
+  if ((rc = hii_extra_outputs(ctx, p, h, ctx->stream))) return rc;
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(cs));
   return RG_OK;
@@ -901,7 +902,7 @@ int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
     int r;
     if ((plain || rec) && (r = copy_grid(ctx, (void*)d.weighted_sfr, h->weighted_sfr, bp, H2D, cs))) return r;
     if (p->Flag_BHFeedback && (r = copy_grid(ctx, (void*)d.effective_bhm, h->effective_bhm, bp, H2D, cs))) return r;
-    if ((r = hii_rec_inputs(ctx, p, h, cs))) return r;
+    if ((r = hii_extra_inputs(ctx, p, h, cs))) return r;
     if ((r = stage_record(ctx, 5, cs, &hs.inputs))) return r;
     if ((r = copy_grid(ctx, d.z_at_ionization, h->z_at_ionization, br, H2D, cs))) return r;
     if ((r = copy_grid(ctx, d.J_21_at_ionization, h->J_21_at_ionization, br, H2D, cs))) return r;
@@ -940,7 +941,7 @@ int rg_reion_step_host(rg_context* ctx, const rg_params* p, const rg_snapshot* s
   if ((rc = copy_grid(ctx, h->z_at_ionization, d.z_at_ionization, br, D2H, co))) return fail(rc);
   if ((rc = copy_grid(ctx, h->J_21_at_ionization, d.J_21_at_ionization, br, D2H, co))) return fail(rc);
   if ((rc = copy_grid(ctx, h->temp_kinetic_all_gas, d.temp_kinetic_all_gas, br, D2H, co))) return fail(rc);
-  if ((rc = hii_rec_outputs(ctx, p, h, co))) return fail(rc);
+  if ((rc = hii_extra_outputs(ctx, p, h, co))) return fail(rc);
   if (h->delta_T) {
     rg_grids dd = d;
     if (vel) dd.vel = ctx->vel_stage;
