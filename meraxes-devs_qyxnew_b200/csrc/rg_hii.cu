@@ -242,7 +242,8 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
   float* rt = reinterpret_cast<float*>(smem + N);
   // ZB shared tiles (with two, grid u + 1 is copied while grid u is transformed); the tile of
   // unit u is the exchange buffer of its transform
-  cf* tiles = reinterpret_cast<cf*>(rt + round_up(NG * ROWS * RP, 4));
+  // (the EXT instantiation lays the tiles out after the row buffers of the grids it has)
+  cf* tiles = reinterpret_cast<cf*>(rt + round_up((EXT ? bt.ng : NG) * ROWS * RP, 4));
   const int x = blockIdx.y, y0 = blockIdx.x * ROWS;
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   const size_t nwords = (size_t)gridDim.x * gridDim.y * W * NTH;
@@ -720,8 +721,9 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   if (rc) return rc;
   using C = Cfg<N>;
   static_assert(HiiZ<N, FINAL>::smem(NG) <= 227 * 1024, "z pass shared memory above the per-block limit");
-  const size_t sm = HiiZ<N, FINAL>::smem(NG);
-  RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL, EXT>, sm));
+  // the EXT instantiation takes the shared memory of the grids it has, not of its maximum
+  const size_t sm = HiiZ<N, FINAL>::smem(EXT ? bt.ng : NG);
+  RG_CUDA_TRY(ctx, prep(k_hii_z<N, NG, FINAL, EXT>, HiiZ<N, FINAL>::smem(NG)));
   const dim3 grid(N / (2 * C::QZ), N);
   // algorithmic bytes: the Hermitian halves of NG grids per radius, z_at_ionization on the
   // first batch; the closing pass writes xH and temperature and reads deltax, weighted_sfr,
