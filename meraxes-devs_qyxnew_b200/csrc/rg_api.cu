@@ -484,7 +484,7 @@ static int find_hii(rg_context* ctx, const rg_params* p, const rg_snapshot* s, c
   if (rc) return rc;
   if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return set_error(ctx, RG_EINVAL, "snapshot out of range");
   if (p->Flag_IncludeRecombinations) {
-    if (!ctx->rec_y)
+    if (!ctx->rec_y || ctx->rec_nz < 1 || ctx->rec_nt < 1 || ctx->rec_ng < 3)
       return set_error(ctx, RG_EINVAL, "Flag_IncludeRecombinations needs rg_set_recombination_tables first");
     if (!g->Gamma12 || !g->N_rec || !g->residual_xH || !g->clumping_factor || !g->t_resp)
       return set_error(ctx, RG_EINVAL, "recombinations need Gamma12, N_rec, residual_xH, clumping_factor, t_resp");
@@ -569,6 +569,7 @@ int rg_set_recombination_tables(rg_context* ctx, const double* lnGamma, int n_z,
   if (ctx->rec_y) cudaFree(ctx->rec_y);
   if (ctx->rec_c) cudaFree(ctx->rec_c);
   ctx->rec_knots = ctx->rec_y = ctx->rec_c = nullptr;
+  ctx->rec_nz = ctx->rec_nt = ctx->rec_ng = 0;
   if (cudaMalloc((void**)&ctx->rec_knots, sizeof(double) * n_gamma) != cudaSuccess ||
       cudaMalloc((void**)&ctx->rec_y, sizeof(double) * 3 * per) != cudaSuccess ||
       cudaMalloc((void**)&ctx->rec_c, sizeof(double) * 3 * per) != cudaSuccess) {
@@ -577,10 +578,18 @@ int rg_set_recombination_tables(rg_context* ctx, const double* lnGamma, int n_z,
     ctx->rec_knots = ctx->rec_y = ctx->rec_c = nullptr;
     return set_error(ctx, RG_ENOMEM, "cudaMalloc of the recombination tables failed");
   }
-  RG_CUDA_TRY(ctx, cudaMemcpy(ctx->rec_knots, lnGamma, sizeof(double) * n_gamma, cudaMemcpyHostToDevice));
-  for (int k = 0; k < 3; ++k)
-    RG_CUDA_TRY(ctx, cudaMemcpy(ctx->rec_y + (size_t)k * per, tabs[k], sizeof(double) * per, cudaMemcpyHostToDevice));
-  RG_CUDA_TRY(ctx, cudaMemcpy(ctx->rec_c, c.data(), sizeof(double) * 3 * per, cudaMemcpyHostToDevice));
+  cudaError_t e = cudaMemcpy(ctx->rec_knots, lnGamma, sizeof(double) * n_gamma, cudaMemcpyHostToDevice);
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+    e = cudaMemcpy(ctx->rec_y + (size_t)k * per, tabs[k], sizeof(double) * per, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->rec_c, c.data(), sizeof(double) * 3 * per, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    // no half-filled tables stay behind: find_HII_bubbles then asks for the tables again
+    cudaFree(ctx->rec_knots);
+    cudaFree(ctx->rec_y);
+    cudaFree(ctx->rec_c);
+    ctx->rec_knots = ctx->rec_y = ctx->rec_c = nullptr;
+    return set_error(ctx, RG_ECUDA, std::string("copying the recombination tables: ") + cudaGetErrorString(e));
+  }
   ctx->rec_nz = n_z;
   ctx->rec_nt = n_t;
   ctx->rec_ng = n_gamma;
