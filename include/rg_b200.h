@@ -319,6 +319,13 @@ int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int m
 int rg_debug_ts_tables(const rg_params* p, const rg_snapshot* s, int n_hist, double x_e_ave,
                        double collapse_fraction, int max_shells, double* shells, double* freq, float* coef);
 
+/* The AGN X-ray band tables of the same engine (Flag_IncludeAGNXray; host only):
+     agn[2][3][14][nS]: band (soft, hard) x kind (heat, ion, lya) frequency integrals per x_e node
+                        (ComputeTs.c:834-897), zero for a band that is off
+     const_zp[3]       : const_zp_prefactor_GAL, _AGN_soft, _AGN_hard (ComputeTs.c:1014-1131) */
+int rg_debug_ts_agn_tables(const rg_params* p, const rg_snapshot* s, int n_hist, double x_e_ave,
+                           double collapse_fraction, int max_shells, double* agn, double* const_zp);
+
 /* ---- allocation-free round trip (no counterpart in the reference) ----
    rg_debug_filter_roundtrip without a context and without any device allocation, for
    callers that cannot allocate: one that has given the device's memory to its own pool,

@@ -773,6 +773,37 @@ int rg_debug_ts_tables(const rg_params* p, const rg_snapshot* s, int n_hist, dou
   return RG_OK;
 }
 
+int rg_debug_ts_agn_tables(const rg_params* p, const rg_snapshot* s, int n_hist, double x_e_ave,
+                           double collapse_fraction, int max_shells, double* agn, double* const_zp) {
+  if (!p || !s || !s->ZZ || !agn || !const_zp || n_hist < 0) return RG_EINVAL;
+  if (s->snapshot < 0 || s->snapshot >= s->n_snapshots) return RG_EINVAL;
+  if (p->Flag_IncludeAGNXray < 0 || p->Flag_IncludeAGNXray > 3) return RG_EINVAL;
+  const int nS = p->TsNumFilterSteps;
+  if (nS < 1 || nS > max_shells) return RG_EINVAL;
+  if (!s->stored_fcoll && s->snapshot > 0) return RG_EINVAL;
+  TsShells sh = ts_shells(p, s->ZZ, s->n_snapshots, s->snapshot, n_hist);
+  if (sh.error) return RG_EINVAL;
+  Tables t;
+  if (!p->TablesForXHeatingDir) return RG_ETABLE;
+  if (!load_tables(p->TablesForXHeatingDir, p->ReionNionPhotPerBary, &t).empty()) return RG_ETABLE;
+  TsTables tb;
+  std::string msg;
+  int rc = ts_tables(p, t, sh, s->ZZ[s->snapshot], x_e_ave, collapse_fraction, s->ZZ, s->stored_fcoll, s->snapshot,
+                     &tb, &msg);
+  if (rc) return rc;
+  for (int b = 0; b < 2; ++b)
+    for (int k = 0; k < 3; ++k)
+      for (int m = 0; m < x_int_NXHII; ++m)
+        for (int r = 0; r < nS; ++r)
+          agn[(((size_t)b * 3 + k) * x_int_NXHII + m) * nS + r] =
+              tb.agn[b][k].empty() ? 0.0 : tb.agn[b][k][(size_t)m * nS + r];
+  const TsPrefactors pf = ts_prefactors(p, s->ZZ[s->snapshot]);
+  const_zp[0] = pf.const_zp_prefactor_GAL;
+  const_zp[1] = pf.const_zp_prefactor_AGN[0];
+  const_zp[2] = pf.const_zp_prefactor_AGN[1];
+  return RG_OK;
+}
+
 int rg_profile_enable(rg_context* ctx, int on) {
   if (!ctx) return RG_EINVAL;
   prof_resolve(ctx);

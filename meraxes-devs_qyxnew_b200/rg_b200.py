@@ -142,6 +142,8 @@ _SIGS = {
     "rg_radius_schedule": (C.c_int, [_P(rg_params), C.c_double, _P(C.c_double), C.c_int, _P(C.c_int)]),
     "rg_debug_ts_tables": (C.c_int, [_P(rg_params), _P(rg_snapshot), C.c_int, C.c_double, C.c_double, C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rg_debug_ts_agn_tables": (C.c_int, [_P(rg_params), _P(rg_snapshot), C.c_int, C.c_double, C.c_double, C.c_int,
+                                         C.c_void_p, C.c_void_p]),
     "rg_filter_roundtrip_noalloc": (C.c_int, [_P(rg_params), C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                               C.c_void_p, C.c_char_p, C.c_size_t]),
 }
@@ -219,6 +221,20 @@ def ts_tables(p: rg_params, zz, snap: int, n_hist: int, x_e_ave: float, collapse
                                           shells.ctypes.data, freq.ctypes.data if with_freq else None,
                                           coef.ctypes.data))
     return shells, freq, coef
+
+
+def ts_agn_tables(p: rg_params, zz, snap: int, n_hist: int, x_e_ave: float, collapse_fraction: float,
+                  stored_fcoll=None):
+    """The AGN band tables [2][3][14][nS] and (const_zp GAL, AGN soft, AGN hard) of the host
+    coefficient engine (no device work)."""
+    import numpy as np
+    ns = p.TsNumFilterSteps
+    agn = np.zeros((2, 3, 14, ns))
+    cz = np.zeros(3)
+    s = snapshot(zz, snap, stored_fcoll)
+    check(None, load().rg_debug_ts_agn_tables(C.byref(p), C.byref(s), n_hist, x_e_ave, collapse_fraction, ns,
+                                              agn.ctypes.data, cz.ctypes.data))
+    return agn, cz
 
 
 def snapshot(zz, snap: int, stored_fcoll=None):

@@ -140,3 +140,33 @@ def test_engine_frequency_tables_match_oracle(engine_case):
         assert np.all(np.abs(got - want) <= 1e-6 * np.abs(want) + 1e-300)
     assert np.allclose(shells[5], sum_lyn, rtol=1e-12, atol=0)
     assert np.all(heat > 0) and np.all(lya > 0)
+
+
+@pytest.mark.parametrize("flag", [1, 2, 3])
+def test_engine_agn_tables_match_oracle(engine_case, flag):
+    """The AGN X-ray band integrals (limits redshifted from zpp to zp, the band's spectral index)
+    and the band prefactors of the library's host engine against the oracle."""
+    p, zz, idx, sf = engine_case
+    p = rg.rg_params.from_buffer_copy(p)
+    p.Flag_IncludeAGNXray = flag
+    p.TablesForXHeatingDir = rg.TABLES_DIR.encode()
+    x_e_ave, cf = 3e-4, 2.5e-4
+    agn, cz = rg.ts_agn_tables(p, zz, idx, idx + 1, x_e_ave, cf, sf)
+    op = oracle_params(p)
+    T = to.TsTables()
+    sh, _ = to.shells_and_sources(op, zz, idx, None, None, [0] * (idx + 1), [0] * (idx + 1), want_grids=False)
+    bands = [b for b, on in ((0, flag in (1, 3)), (1, flag in (1, 2))) if on]
+    ft = to.freq_tables(op, T, sh, zz[idx], x_e_ave, cf, zz, sf, idx, agn_bands=tuple(bands))
+    for b in (0, 1):
+        for k in range(3):
+            if b in bands:
+                want = ft[4][b][k]
+                assert np.all(np.abs(agn[b, k] - want) <= 1e-6 * np.abs(want) + 1e-300), (b, k)
+                assert np.any(want != 0)
+            else:
+                assert np.all(agn[b, k] == 0)
+    pf = to.prefactors(op, float(zz[idx]))
+    assert cz[0] == pytest.approx(pf["const_zp"], rel=1e-12)
+    assert cz[1] == pytest.approx(pf["const_agn"][0], rel=1e-12)
+    assert cz[2] == pytest.approx(pf["const_agn"][1], rel=1e-12)
+
