@@ -334,7 +334,8 @@ int rg_debug_ts_agn_tables(const rg_params* p, const rg_snapshot* s, int n_hist,
    to RG_NOALLOC_MAX_GRID_DIM; larger ReionGridDim values return RG_EUNSUPPORTED with the
    reason in errbuf.  Runs on the current device, on `stream` (a cudaStream_t; NULL = the
    default stream), asynchronously.  The first call on a device looks up the array's address
-   (once per device); make it before any stream capture begins.  Nothing in the scratch has
+   (once per device and CUDA context: after cudaDeviceReset the next call looks it up again);
+   make the first call, and the first after a reset, before any stream capture begins.  Nothing in the scratch has
    to start at zero.  Two calls in flight at once on one device race on the scratch: order
    them (one stream, or the caller's own synchronisation).  errbuf (may be NULL) receives
    a message when the status is not RG_OK. */

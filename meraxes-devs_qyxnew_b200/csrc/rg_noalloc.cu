@@ -13,11 +13,16 @@
 //   was written earlier in the same call.
 //
 // Set-up: the first call on a device (with that device current) looks up the array's
-// device address with cudaGetSymbolAddress and caches it; later calls reuse it.  Make the
-// first call on each device before any stream capture begins.
+// device address with cudaGetSymbolAddress and caches it together with the CUDA context it
+// belongs to; later calls in the same context reuse it.  After cudaDeviceReset (or any
+// other way the device's primary context is destroyed and made anew) the next call sees a
+// different context and looks the address up again, so a stale address is never used.
+// Make the first call on each device, and the first after a reset, before any stream
+// capture begins.
 //
 // Two calls in flight at the same time on one device (different streams, or different
 // host threads) share the scratch and race: the caller orders them, e.g. on one stream.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -45,6 +50,24 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[RG_NOALLOC_SCRATCH_BYT
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_na_mutex;
 void* g_na_base[NA_MAX_DEVICES] = {};
+CUcontext g_na_ctx[NA_MAX_DEVICES] = {};
+
+// the current driver context, through the runtime's driver entry point (no link-time
+// dependency on libcuda); nullptr when it cannot be had, which forces a fresh look-up
+CUcontext na_current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<Fn>(f);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
 
 // twiddles computed on the device in double, rounded to float (the host table of the
 // context path is cos/sin in double rounded to float: the same values up to the last bit of
@@ -167,12 +190,16 @@ extern "C" int rg_filter_roundtrip_noalloc(const rg_params* p, const float* d_in
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_base[dev]) {
-      const cudaError_t e = cudaGetSymbolAddress(&g_na_base[dev], g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        g_na_base[dev] = nullptr;
-        return na_fail(errbuf, errlen, RG_ECUDA, cudaGetErrorString(e));
-      }
+    const CUcontext cur = na_current_context();
+    if (!g_na_base[dev] || !cur || cur != g_na_ctx[dev]) {
+      g_na_base[dev] = nullptr;
+      g_na_ctx[dev] = nullptr;
+      void* addr = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+      if (e != cudaSuccess) return na_fail(errbuf, errlen, RG_ECUDA, cudaGetErrorString(e));
+      // cudaGetSymbolAddress makes the primary context current if none was: read it again
+      g_na_ctx[dev] = na_current_context();
+      g_na_base[dev] = addr;
     }
     base = g_na_base[dev];
   }

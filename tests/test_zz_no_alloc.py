@@ -25,7 +25,7 @@ def _noalloc(p, d_in, d_out, R, ftype, stream=None):
     return rc, err.value.decode()
 
 
-@pytest.mark.parametrize("n,box", [(16, 20.0), (32, 40.0), (48, 48.0), (64, 80.0)])
+@pytest.mark.parametrize("n,box", [(8, 10.0), (16, 20.0), (24, 30.0), (32, 40.0), (48, 48.0), (64, 80.0)])
 @pytest.mark.parametrize("ftype", [-1, 0, 1, 2])
 def test_noalloc_matches_context_path_twice(n, box, ftype):
     import torch
@@ -76,6 +76,10 @@ def test_noalloc_allocates_nothing_and_rejects_large_grids():
     assert rc == rg.RG_EUNSUPPORTED and "RG_NOALLOC_MAX_GRID_DIM" in msg and "64" in msg
     rc, msg = _noalloc(p, d_in, d_out, 5.0, 3)
     assert rc == rg.RG_EINVAL and msg
+    # errbuf may be NULL: the status alone reports the rejection
+    rc = rg.load().rg_filter_roundtrip_noalloc(C.byref(big), d_big.data_ptr(), d_big.data_ptr(), 5.0, 0, None,
+                                                None, 0)
+    assert rc == rg.RG_EUNSUPPORTED
 
 
 def _pad_mask(n):
