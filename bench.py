@@ -45,6 +45,7 @@ import numpy as np  # noqa: E402
 import workloads as wl  # noqa: E402
 
 METRIC = "ms/snapshot find_HII_bubbles+Ts at 256^3/512^3"
+DATA_DESC = "synthetic (seeded generators at the workload's shapes and sizes)"
 DEFAULT_CONFIG = "c4_512"
 
 
@@ -199,110 +200,167 @@ def make_inputs(cfg, rank, zz, snap, n_hist):
 # ---------------------------------------------------------------------------
 # CPU restatement on bounded samples
 
-def cpu_sample(cfg, src, ti, zz, snap, radii: int = 1, shells: int = 1, table_shells: int = 2,
-               cell_planes: int = 0):
-    """Time the oracle (float32 pocketfft on all host cores) on a bounded sample of one
-    snapshot and extrapolate to the whole snapshot:
-      find_HII_bubbles: forward r2c of every grid, ``radii`` of the nR radii, closing pass;
-      ComputeTs: ``shells`` of the nS shells (FFTs, filter, sums), the frequency tables of
-      ``table_shells`` shells, and the per-cell update on ``cell_planes`` x-planes;
-      delta_T in full.  Returns (ms per snapshot, description, wall seconds)."""
+def oracle_history_slots(cfg, zz, snap):
+    """History slots the shells read, from the oracle's own shell schedule (no library call)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import reion_oracle as ro
-    import tables
-    ro.set_recfast(tables.Recfast(tables.default_tables_dir()).T)
-    p = oracle_params(cfg)
-    n = cfg.n
-    U = wl.from_padded
-    wall0 = time.perf_counter()
-    st = ro.HIIState.fresh(n)
-    xe = U(ti.x_e_box_prev) if ti is not None else None
-    tk = ti.Tk_box if ti is not None else None
-    _, _, _, diag = ro.find_hii_bubbles(p, cfg.z, src.deltax, src.stars, src.sfr, st, "fp32",
-                                        x_e_box=xe, Tk_box=tk, radius_subset=radii, with_dead_grids=True)
-    nr = diag["n_radii"]
-    t = diag["timing"]
-    est = t["forward"] + t["per_radius"] * nr + t["final"]
-    desc = f"find_HII_bubbles: forward r2c + {radii} of {nr} radii + closing pass, extrapolated to {nr} radii"
-    if ti is not None:
-        import ts_oracle as to
-        T = to.TsTables()
-        to.gk61_rule()                 # the quadrature rule is set up once, outside the timed parts
-        cm = to.Cosmo(p)
-        zp = float(zz[snap])
-        nS = p.TsNumFilterSteps
-        planes = cell_planes or max(1, n // 64)
-        xprev = U(ti.x_e_box_prev)
-        # history re-weighting of the source grids (elementwise): timed on `planes` x-planes
+    import ts_oracle as to
+    sh, _ = to.shells_and_sources(oracle_params(cfg), zz, snap, None, None, None, None, want_grids=False)
+    return sh.max_slot + 1
+
+
+class CpuSampler:
+    """The oracle (float32 pocketfft on all host cores) timed on bounded samples of one snapshot.
+
+    ``fixed()`` times, once, the parts that run once per snapshot: the forward r2c of every
+    find_HII grid and the closing pass; ComputeTs' history re-weighting and per-cell update on a
+    few x-planes (scaled by N / planes), the frequency tables of two shells (scaled by nS / 2),
+    the x_e interpolation nodes; delta_T in full.  ``sample(i)`` times one radius of the
+    excursion set (window, inverse FFTs, barrier test; successive radius samples walk the schedule
+    in steps of 7) or, on odd i with ComputeTs, one Ts shell (r2c, filter, c2r, sums; shells in
+    steps of 3).  A snapshot's estimate is fixed + nR x mean radius + nS x mean shell."""
+
+    def __init__(self, cfg, src, ti, zz, snap):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import reion_oracle as ro
+        import tables
+        ro.set_recfast(tables.Recfast(tables.default_tables_dir()).T)
+        self.ro = ro
+        self.cfg, self.src, self.ti, self.zz, self.snap = cfg, src, ti, zz, snap
+        self.p = oracle_params(cfg)
+        self.n = cfg.n
+        self.nr = len(ro.radius_schedule(self.p, cfg.z))
+        self.nS = self.p.TsNumFilterSteps if cfg.spin_temp else 0
+        self.spectra = None
+        self.fixed_s = None
+        self.desc = ""
+        self.radius_s, self.shell_s = [], []
+
+    def _hii(self, **kw):
+        ro, src, ti, n = self.ro, self.src, self.ti, self.n
+        st = ro.HIIState.fresh(n)
+        xe = wl.from_padded(ti.x_e_box_prev) if ti is not None else None
+        tk = ti.Tk_box if ti is not None else None
+        return ro.find_hii_bubbles(self.p, self.cfg.z, src.deltax, src.stars, src.sfr, st, "fp32",
+                                   x_e_box=xe, Tk_box=tk, with_dead_grids=True, **kw)
+
+    def fixed(self, planes: int = 0, table_shells: int = 2):
+        ro, src, ti, n, U = self.ro, self.src, self.ti, self.n, wl.from_padded
+        parts = {}
+        _, _, _, d = self._hii(radius_indices=(), skip_final=True)
+        parts["hii_forward"] = d["timing"]["forward"]
+        self.spectra = d["spectra"]
         t0 = time.perf_counter()
-        sh, _ = to.shells_and_sources(p, zz, snap, U(src.sfr)[:planes], U(src.xray)[:planes],
-                                      [U(a)[:planes] for a in ti.sfr_histories],
-                                      [U(a)[:planes] for a in ti.xray_histories])
-        t_setup = (time.perf_counter() - t0) * n / planes
-        # frequency tables of table_shells shells
-        sub = to.Shells()
-        for k in ("R", "zpp_edge", "zpp", "dzpp", "dt_dzpp"):
-            setattr(sub, k, getattr(sh, k)[:table_shells])
-        sub.final_weight = sh.final_weight
+        self._hii(radius_indices=(), spectra_in=self.spectra)
+        parts["hii_closing_pass"] = time.perf_counter() - t0
+        desc = [f"find_HII_bubbles: forward r2c + closing pass once, 1 of {self.nr} radii per sample x {self.nr}"]
+        if ti is not None:
+            import ts_oracle as to
+            self.to = to
+            p, zz, snap = self.p, self.zz, self.snap
+            self.T = to.TsTables()
+            to.gk61_rule()                 # the quadrature rule is set up once, outside the timed parts
+            cm = to.Cosmo(p)
+            self.zp = zp = float(zz[snap])
+            nS = self.nS
+            planes = planes or max(1, n // 64)
+            xprev = U(ti.x_e_box_prev)
+            t0 = time.perf_counter()
+            sh, _ = to.shells_and_sources(p, zz, snap, U(src.sfr)[:planes], U(src.xray)[:planes],
+                                          [U(a)[:planes] for a in ti.sfr_histories],
+                                          [U(a)[:planes] for a in ti.xray_histories])
+            parts["ts_history_reweighting"] = (time.perf_counter() - t0) * n / planes
+            self.sh = sh
+            sub = to.Shells()
+            for k in ("R", "zpp_edge", "zpp", "dzpp", "dt_dzpp"):
+                setattr(sub, k, getattr(sh, k)[:table_shells])
+            sub.final_weight = sh.final_weight
+            t0 = time.perf_counter()
+            heat, ion, lya, sum_lyn = to.freq_tables(p, self.T, sub, zp, float(np.mean(xprev)), 1e-3, zz,
+                                                     ti.stored_fcoll, snap)
+            parts["ts_frequency_tables"] = (time.perf_counter() - t0) * nS / table_shells
+            self.tabs = tuple(np.repeat(a[:, :1], nS, axis=1) for a in (heat, ion, lya))
+            self.lyn = np.repeat(sum_lyn[:1], nS)
+            t0 = time.perf_counter()
+            self.xi = to.xe_interp_index(self.T, xprev)
+            parts["ts_xe_nodes"] = time.perf_counter() - t0
+            sums = [np.zeros((planes, n, n)) for _ in range(4)]
+            pf = to.prefactors(p, zp)
+            d = U(src.deltax)[:planes]
+            t0 = time.perf_counter()
+            to.finish_sums(p, cm, pf, zp, d, sums)
+            to.evolve_cells(p, cm, self.T, pf, zp, zp - float(zz[snap - 1]), d, xprev[:planes], ti.Tk_box[:planes],
+                            sums)
+            parts["ts_per_cell_update"] = (time.perf_counter() - t0) * n / planes
+            t0 = time.perf_counter()
+            ro.delta_T(p, self.cfg.z, np.full((n, n, n), 0.5, np.float32), U(src.deltax), ti.Tk_box)
+            parts["delta_T"] = time.perf_counter() - t0
+            self.sums = [np.zeros((n, n, n)) for _ in range(4)]
+            desc.append(f"ComputeTs: history re-weighting and per-cell update on {planes} of {n} x-planes "
+                        f"x {n / planes:g}, frequency tables of {table_shells} shells x {nS / table_shells:g}, "
+                        f"1 of {nS} shells (r2c, filter, c2r, sums) per sample x {nS}; delta_T in full once")
+        self.fixed_s = parts
+        self.desc = "; ".join(desc)
+        return parts
+
+    def sample(self, i: int):
+        """One radius (even i, or every i without ComputeTs) or one Ts shell (odd i).  Returns the
+        wall seconds of the sample; ``estimate()`` combines the samples taken so far."""
         t0 = time.perf_counter()
-        heat, ion, lya, sum_lyn = to.freq_tables(p, T, sub, zp, float(np.mean(xprev)), 1e-3, zz, ti.stored_fcoll,
-                                                 snap)
-        t_tab = (time.perf_counter() - t0) * nS / table_shells
-        tabs = tuple(np.repeat(a[:, :1], nS, axis=1) for a in (heat, ion, lya))
-        lyn = np.repeat(sum_lyn[:1], nS)
-        # x_e interpolation nodes (once per snapshot), then `shells` filtered shells in full
-        t0 = time.perf_counter()
-        xi = to.xe_interp_index(T, xprev)
-        sums = [np.zeros(xprev.shape) for _ in range(4)]
-        t_xi = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        for r in range(shells):
-            to.shell_accumulate(p, sh, r + 1, U(src.sfr), U(src.xray), xi, tabs, lyn, zp, sums, "fp32")
-        t_shell = (time.perf_counter() - t0) / shells * nS
-        # the per-cell update on `planes` x-planes
-        pf = to.prefactors(p, zp)
-        d = U(src.deltax)[:planes]
-        part = [a[:planes] for a in sums]
-        t0 = time.perf_counter()
-        to.finish_sums(p, cm, pf, zp, d, part)
-        to.evolve_cells(p, cm, T, pf, zp, zp - float(zz[snap - 1]), d, xprev[:planes], ti.Tk_box[:planes], part)
-        t_cell = (time.perf_counter() - t0) * n / planes
-        del sums, xi
-        est += t_setup + t_tab + t_xi + t_shell + t_cell
-        desc += (f"; ComputeTs: history re-weighting on {planes} of {n} planes x {n / planes:g}, frequency "
-                 f"tables of {table_shells} shells x {nS / table_shells:g}, {shells} of {nS} shells "
-                 f"(r2c, filter, c2r, sums) x {nS}, per-cell update on {planes} of {n} planes x {n / planes:g}")
-        t0 = time.perf_counter()
-        ro.delta_T(p, cfg.z, np.full((n, n, n), 0.5, np.float32), U(src.deltax), ti.Tk_box)
-        est += time.perf_counter() - t0
-        desc += "; delta_T in full"
-    return est * 1e3, desc, time.perf_counter() - wall0, nr
+        if not self.nS or i % 2 == 0:
+            ir = ((i // 2 if self.nS else i) * 7) % self.nr
+            _, _, _, d = self._hii(radius_indices=(ir,), spectra_in=self.spectra, skip_final=True)
+            self.radius_s.append(d["timing"]["per_radius"])
+        else:
+            U = wl.from_padded
+            r = 1 + ((i // 2) * 3) % (self.nS - 1) if self.nS > 1 else 0
+            t1 = time.perf_counter()
+            self.to.shell_accumulate(self.p, self.sh, r, U(self.src.sfr), U(self.src.xray), self.xi, self.tabs,
+                                     self.lyn, self.zp, self.sums, "fp32")
+            self.shell_s.append(time.perf_counter() - t1)
+        return time.perf_counter() - t0
+
+    def estimate(self):
+        """ms per snapshot: fixed parts + nR x mean radius + nS x mean shell."""
+        t_r = statistics.mean(self.radius_s)
+        t_s = statistics.mean(self.shell_s) if self.nS else 0.0
+        return (sum(self.fixed_s.values()) + self.nr * t_r + self.nS * t_s) * 1e3
 
 
 def run_reference(args, cfg):
+    """The reference arm: the CPU restatement of the reference algorithm (the oracle), rank 0 only.
+    It loads nothing of the library."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     zz, snap = wl.snapshot_redshifts(cfg.z)
-    n_hist = snap + 1 if cfg.spin_temp else 0
-    if cfg.spin_temp:
-        import rg_b200 as rg
-        n_hist = history_slots(cfg, rg, zz, snap)
+    n_hist = oracle_history_slots(cfg, zz, snap) if cfg.spin_temp else 0
     src, ti = make_inputs(cfg, 0, zz, snap, n_hist)
-    vals = []
-    nr, desc = 0, ""
-    for i in range(args.warmup + args.steps):
-        ms, desc, wall, nr = cpu_sample(cfg, src, ti, zz, snap)
-        if i >= args.warmup:
-            vals.append(ms)
-    v = statistics.mean(vals)
+    cs = CpuSampler(cfg, src, ti, zz, snap)
+    w0 = time.perf_counter()
+    cs.fixed()
+    fixed_wall = time.perf_counter() - w0
+    walls = []
+    for i in range(args.warmup):
+        cs.sample(i)
+    cs.radius_s, cs.shell_s = [], []
+    for i in range(args.warmup, args.warmup + args.steps):
+        walls.append(cs.sample(i))
+    if not cs.radius_s or (cs.nS and not cs.shell_s):
+        cs.sample(0 if not cs.radius_s else 1)        # fewer than two timed steps: one more sample
+    v = cs.estimate()
+    sample_ms = statistics.mean(walls) * 1e3
+    desc = (cs.desc + f"; each timed step is one sample, a radius or a shell in turn ({sample_ms / 1e3:.2f} s "
+            f"wall on average), the snapshot value is extrapolated from the samples and the once-per-snapshot "
+            f"parts ({fixed_wall:.1f} s wall, timed before the warm-up); oracle restatement, scipy pocketfft "
+            "float32, all host cores (the reference needs FFTW/GSL/MPI, absent here)")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/snapshot", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-            "config": workload_desc(cfg, nr),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA_DESC,
+            "config": workload_desc(cfg, cs.nr), "extrapolated": True,
+            "fixed_parts_s": cs.fixed_s, "radius_sample_s": statistics.mean(cs.radius_s),
+            "shell_sample_s": statistics.mean(cs.shell_s) if cs.shell_s else None,
             "cpu_baseline": {"value": v, "unit": "ms/snapshot", "cores": os.cpu_count(), "kind": "port",
-                             "sample": desc + "; oracle restatement, scipy pocketfft float32, all host cores "
-                                              "(the reference needs FFTW/GSL/MPI, absent here)"},
+                             "sample": desc},
             "e2e": {"value": v, "unit": "ms/snapshot", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -661,14 +719,20 @@ def run_ours(args, cfg):
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        ms_cpu, desc, wall, _ = cpu_sample(cfg, src, ti, zz, snap)
+        w0 = time.perf_counter()
+        cs = CpuSampler(cfg, src, ti, zz, snap)
+        cs.fixed()
+        for i in range(2):
+            cs.sample(i)
+        ms_cpu = cs.estimate()
         cpu = {"value": ms_cpu, "unit": "ms/snapshot", "cores": os.cpu_count(), "kind": "port",
-               "sample": desc + f"; oracle restatement, scipy pocketfft float32 on all host cores ({wall:.1f} s wall)"}
+               "sample": cs.desc + f"; two samples; oracle restatement, scipy pocketfft float32 on all host cores "
+                                   f"({time.perf_counter() - w0:.1f} s wall)"}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "ms/snapshot", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators at the workload's shapes and sizes)",
-                "config": dict(workload_desc(cfg, nr), mode=args.mode, parallelism=f"replicas x{ws}"),
+                "vs_baseline": None, "dtype": "f32", "data": DATA_DESC,
+                "config": workload_desc(cfg, nr), "mode": args.mode, "parallelism": f"replicas x{ws}",
                 "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clk, "results": results, "extras": extras}
         print(json.dumps(line), flush=True)

@@ -320,7 +320,8 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
                      effective_bhar: np.ndarray | None = None, record_margins: bool = False,
                      radius_subset: int | None = None, with_dead_grids: bool = False, rec_tables=None,
                      prev_z: float | None = None, starsIII: np.ndarray | None = None,
-                     weighted_sfrIII: np.ndarray | None = None):
+                     weighted_sfrIII: np.ndarray | None = None, spectra_in: dict | None = None,
+                     radius_indices=None, skip_final: bool = False):
     """Restatement of _find_HII_bubbles() (find_HII_bubbles.c:86-710), one rank.
 
     With ``Flag_IncludeRecombinations`` the state carries Gamma12 and N_rec, ``rec_tables`` is a
@@ -344,6 +345,11 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     the reference's).  ``with_dead_grids`` also transforms weighted_sfr every
     radius as the reference does, although without recombinations nothing reads
     the result (used when timing the CPU baseline).
+
+    Timing hooks for the CPU baseline (the outputs are then partial): ``spectra_in``
+    reuses the forward spectra of an earlier call (``diag["spectra"]``) instead of
+    transforming again, ``radius_indices`` runs only those radii of the schedule, and
+    ``skip_final`` returns before the closing pass.
     """
     import time as _time
     t_start = _time.perf_counter()
@@ -385,7 +391,10 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
             grids["wsfrIII"] = weighted_sfrIII[:, :, :n]
     if with_dead_grids:
         grids["wsfr"] = weighted_sfr[:, :, :n]
-    spectra = {k: forward(v, precision) for k, v in grids.items()}
+    if spectra_in is not None:
+        spectra = spectra_in
+    else:
+        spectra = {k: forward(v, precision) for k, v in grids.items()}
     t_forward = _time.perf_counter() - t_start
     radius_times = []
 
@@ -396,6 +405,8 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     sched = radius_schedule(p, z)
     for ir, (R, last) in enumerate(sched):
         if radius_subset is not None and ir >= radius_subset and not last:
+            continue
+        if radius_indices is not None and ir not in radius_indices:
             continue
         t_r0 = _time.perf_counter()
         filt = {}
@@ -505,6 +516,12 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
 
         radius_times.append(_time.perf_counter() - t_r0)
 
+    if skip_final:
+        diag = {"n_radii": len(sched), "spectra": spectra,
+                "timing": {"forward": t_forward, "per_radius": float(np.mean(radius_times)) if radius_times else 0.0,
+                           "final": 0.0}}
+        return xH, r_bubble, {}, diag
+
     # final pass (find_HII_bubbles.c:577-702)
     t_f0 = _time.perf_counter()
     dxu = dx_real.astype(f32)
@@ -564,7 +581,8 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
         s["mass_weighted_global_r_bubble"] = (r_bubble.astype(np.float64) * dom).sum() / mw
     t_final = _time.perf_counter() - t_f0
     diag = {"min_margin": min_margin, "first_cross": first_cross, "n_radii": len(sched), "rec": rec_out,
-            "timing": {"forward": t_forward, "per_radius": float(np.mean(radius_times)), "final": t_final}}
+            "timing": {"forward": t_forward, "per_radius": float(np.mean(radius_times)) if radius_times else 0.0,
+                       "final": t_final}, "spectra": spectra}
     return xH, r_bubble, s, diag
 
 

@@ -423,7 +423,8 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
                        extra=()):
     """Returns (Shells, per-shell list of (sfr, xray, *extra) float32 grids or None).  ``extra`` holds
     (grid, histories) pairs re-weighted like the sfr grids: the AGN emissivity bands
-    (load_reion_bh_grids)."""
+    (load_reion_bh_grids).  ``Shells.max_slot`` is the highest history slot the shells read (-1:
+    none); with ``want_grids=False`` the histories may be None (the schedule alone)."""
     cm = Cosmo(p)
     nS = p.TsNumFilterSteps
     box = p.BoxSize / p.Hubble_h
@@ -435,6 +436,7 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
     R = L_FACTOR * box / float(f32(n))
     R_factor = (R_XLy_MAX / R) ** float(f32(1) / f32(nS))   # 1 / (float)nS is a float quotient
     sh = Shells()
+    sh.max_slot = -1
     sh.R = np.zeros(nS)
     sh.zpp_edge = np.zeros(nS)
     scb = np.zeros(nS, np.int64)
@@ -444,6 +446,9 @@ def shells_and_sources(p: ro.Params, ZZ, snapshot: int, sfr, xray, sfr_hist, xra
 
     def load(idx, weight, new_load):
         nonlocal cur
+        sh.max_slot = max(sh.max_slot, int(idx))
+        if sfr_hist is None:          # schedule only: which history slots the shells read
+            return
         if idx < 0 or idx >= len(sfr_hist):
             raise ValueError("history slot %d missing" % idx)
         if not want_grids:
