@@ -74,3 +74,13 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# Measured errors of the GPU outputs against FP64, collected by the configuration-level parity
+# tests and written as a markdown table at the end of the session when RG_PARITY_TABLE names a
+# file (tests/conftest.py).
+PARITY_ROWS: list = []
+
+
+def record(config: str, output: str, measure: str, value: float, gate: str):
+    PARITY_ROWS.append((config, output, measure, float(value), gate))
