@@ -50,6 +50,12 @@ REL_TOL = np.float32(1e-5)
 ABS_TOL = np.float32(1e-8)
 SIGMA_HI = 6.3e-18
 L_FACTOR = 0.620350491
+# The aliasing clamps of find_HII_bubbles.c:377,410 are float constants: fmaxf(x, -1 + REL_TOL)
+# evaluates -1 + REL_TOL in float (-0.99998999), and fminf(x, 0.999) rounds 0.999 to float.  The
+# FP64 form keeps these constants (they define the algorithm; 1 + delta at the floor is 1.00136e-5,
+# not 1e-5) and evaluates everything else in double.
+CLAMP_DELTAX = float(np.float32(-1) + REL_TOL)
+CLAMP_XE = float(np.float32(0.999))
 
 
 @dataclasses.dataclass
@@ -421,7 +427,7 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
             fs = np.maximum(filt["stars"], f32(0)).astype(f32)
             fs = np.where(fs < ABS_TOL, f32(0), fs)
         else:
-            fd = np.maximum(fd, -1 + float(REL_TOL))
+            fd = np.maximum(fd, CLAMP_DELTAX)
             fs = np.maximum(filt["stars"], 0.0)
             fs = np.where(fs < float(ABS_TOL), 0.0, fs)
         if p.Flag_IncludeSpinTemp:
@@ -431,7 +437,7 @@ def find_hii_bubbles(p: Params, z: float, deltax: np.ndarray, stars: np.ndarray,
                 fx = np.where(fx < ABS_TOL, f32(0), fx)
                 fx = np.minimum(fx, f32(0.999)).astype(f32)
             else:
-                fx = np.minimum(np.where(np.maximum(fx, 0.0) < float(ABS_TOL), 0.0, np.maximum(fx, 0.0)), 0.999)
+                fx = np.minimum(np.where(np.maximum(fx, 0.0) < float(ABS_TOL), 0.0, np.maximum(fx, 0.0)), CLAMP_XE)
             neutral = 1.0 - fx.astype(np.float64)
         else:
             neutral = np.ones((n, n, n))

@@ -8,6 +8,13 @@ find_HII_bubbles.c:48-84 run on the host through the oracle's own functions on t
 need them.  It exists because the numpy oracle takes tens of minutes at 512^3; at every size it
 can afford, ``tests/test_gpu_configs.py`` checks it against the numpy oracle first, and it is
 never the thing measured.
+
+Besides the oracle's barrier margins it marks the cells whose ionisation decision is fragile in
+float arithmetic (``diag["fp32_fragile"]``): at some radius, moving each filtered field by its
+FP32 error bound (FRAGILE_REL x its rms) can put the cell on either side of the barrier.  These
+are mostly cells where the filtered density is close to -1, so that 1 + delta, the denominator of
+the collapse fraction, has few correct digits in float; any FP32 evaluation, the reference's own
+included, can decide them either way.
 """
 
 from __future__ import annotations
@@ -17,6 +24,12 @@ import math
 import numpy as np
 
 import reion_oracle as ro
+
+
+# The FP32 error bound of a filtered field, relative to its rms over the box: the float
+# transforms' rounding (about log2(N^3) roundings of 2^-24 each, summed in quadrature) with a
+# safety factor of about 4.
+FRAGILE_REL = 1e-6
 
 
 def _kmag(torch, n, box, dev):
@@ -70,6 +83,7 @@ def find_hii_fp64(p: ro.Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     z_in = T(state.z_at_ionization)
     J21 = T(state.J_21_at_ionization)
     min_margin = torch.full((n, n, n), math.inf, dtype=torch.float64, device=dev)
+    fragile = torch.zeros((n, n, n), dtype=torch.bool, device=dev)
     first_cross = torch.full((n, n, n), -1, dtype=torch.int16, device=dev)
     temp = state.temp_kinetic_all_gas
     rel_tol = float(ro.REL_TOL)
@@ -81,16 +95,26 @@ def find_hii_fp64(p: ro.Params, z: float, deltax: np.ndarray, stars: np.ndarray,
         filt = {}
         for k, s in spectra.items():
             filt[k] = torch.fft.irfftn(s if w is None else s * w, s=(n, n, n), norm="forward")
-        fd = torch.clamp(filt["deltax"], min=-1 + rel_tol)
-        fs = torch.clamp(filt["stars"], min=0.0)
-        fs = torch.where(fs < abs_tol, torch.zeros_like(fs), fs)
+        # FP32 error bound of each filtered field at this radius (FRAGILE_REL x its rms)
+        err = {k: FRAGILE_REL * float(torch.sqrt(torch.mean(v * v))) for k, v in filt.items()}
+        clamp_d = lambda v: torch.clamp(v, min=ro.CLAMP_DELTAX)
+
+        def clamp_s(v):
+            v = torch.clamp(v, min=0.0)
+            return torch.where(v < abs_tol, torch.zeros_like(v), v)
+
+        def clamp_x(v):
+            return torch.clamp(clamp_s(v), max=ro.CLAMP_XE)
+
+        fd = clamp_d(filt["deltax"])
+        fs = clamp_s(filt["stars"])
         if p.Flag_IncludeSpinTemp:
-            fx = torch.clamp(filt["x_e"], min=0.0)
-            fx = torch.clamp(torch.where(fx < abs_tol, torch.zeros_like(fx), fx), max=0.999)
+            fx = clamp_x(filt["x_e"])
             neutral = 1.0 - fx
+            n_lo, n_hi = 1.0 - clamp_x(filt["x_e"] + err["x_e"]), 1.0 - clamp_x(filt["x_e"] - err["x_e"])
         else:
             neutral = torch.ones_like(fd)
-        del filt
+            n_lo = n_hi = neutral
         M_mean = ro.rtom(p, R)
         g_pref = ((1.0 + z) * (1.0 + z) * R * p.UnitLength_in_cm / pixel_volume * p.UnitLength_in_cm ** -3.0)
         g_pref *= (p.UnitMass_in_g / u.UnitTime_in_s) / ro.PROTONMASS * p.ReionNionPhotPerBary
@@ -100,6 +124,12 @@ def find_hii_fp64(p: ro.Params, z: float, deltax: np.ndarray, stars: np.ndarray,
         lhs = (fs / dom) * fcoll_pref
         rhs = neutral
         ion = lhs > rhs
+        # the decision is fragile where the filtered fields moved by their FP32 error bound can
+        # land on either side of the barrier
+        lhs_hi = clamp_s(filt["stars"] + err["stars"]) / (1.0 + clamp_d(filt["deltax"] - err["deltax"])) * fcoll_pref
+        lhs_lo = clamp_s(filt["stars"] - err["stars"]) / (1.0 + clamp_d(filt["deltax"] + err["deltax"])) * fcoll_pref
+        fragile |= ~((lhs_hi <= n_lo) | (lhs_lo > n_hi))
+        del filt, lhs_hi, lhs_lo
         torch.minimum(min_margin, torch.abs(lhs / rhs - 1.0), out=min_margin)
         first_cross[ion & (first_cross < 0)] = ir
         xH[ion] = 0
@@ -143,5 +173,5 @@ def find_hii_fp64(p: ro.Params, z: float, deltax: np.ndarray, stars: np.ndarray,
     s["mass_weighted_global_xH"] = (xH_h.astype(np.float64) * dom).sum() / mw
     s["mass_weighted_global_temp_kinetic_all_gas"] = (temp.astype(np.float64) * dom).sum() / mw
     diag = {"min_margin": min_margin.cpu().numpy(), "first_cross": first_cross.cpu().numpy(),
-            "n_radii": len(sched)}
+            "n_radii": len(sched), "fp32_fragile": fragile.cpu().numpy()}
     return xH_h, r_bubble, s, diag

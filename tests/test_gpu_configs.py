@@ -90,6 +90,9 @@ def compare_hii(tag, res, out, want, n):
     record(tag, "ionised flag", "near-threshold share of disagreements",
            (near[dis].mean() if dis.any() else 1.0), "= 1")
     record(tag, "ionised flag", "cells within 1e-4 of the threshold / N^3", near.sum() / n3, "(reported)")
+    if "fp32_fragile" in diag:
+        record(tag, "ionised flag", "cells whose decision is fragile in float / N^3",
+               diag["fp32_fragile"].sum() / n3, "(reported)")
     assert dis.mean() <= 1e-4
     if dis.any():
         assert np.all(near[dis]), np.max(diag["min_margin"][dis])
@@ -351,3 +354,83 @@ def test_c4_512_filtered_fields():
     cfg = wl.CONFIGS["c4_512"]
     src = wl.make_sources(cfg.n, cfg.box, cfg.seed, cfg.source_scale)
     filtered_field_errors("c4_512 filter 0", cfg, src, 0, ("deltax", "stars"))
+
+
+# ---------------------------------------------------------------------------
+# the GPU against the reference's own C code (oracle/_ref, built from the reference sources)
+
+def _ref_lib():
+    import ref_lib
+    if not ref_lib.available(False):
+        pytest.skip("oracle/_ref is not built")
+    return ref_lib
+
+
+@pytest.mark.parametrize("ftype", [0, 1, 2])
+def test_c0_64_find_hii_against_reference_code(ftype):
+    """c0_64's grid, box and redshift at an efficiency that ionises part of the box: the GPU's
+    find_HII_bubbles against the reference's compiled _find_HII_bubbles on the same inputs (the
+    reference computes in float, so the gates are the FP64 ones with the FP64 oracle's margins)."""
+    ref_lib = _ref_lib()
+    cfg = wl.CONFIGS["c0_64"]
+    n = cfg.n
+    src = wl.make_sources(cfg.n, cfg.box, cfg.seed, cfg.source_scale)
+    p = hii_params(cfg, 4000.0, ftype)
+    res, out = gpu_hii(p, n, cfg.z, src)
+    zz, snap = wl.snapshot_redshifts(cfg.z)
+    ref = ref_lib.run_step(oracle_params(p), zz, snap, {"deltax": src.deltax, "stars": src.stars,
+                                                         "weighted_sfr": src.sfr})
+    diag = fp64_hii(p, cfg.z, src, numpy_oracle=True)[3]
+    near = diag["min_margin"] <= 1e-4
+    tag = f"c0_64 filter {ftype} eff 4000 vs reference code"
+    xr = ref["xH"].reshape(n, n, n)
+    dis = (res["xH"] < ro.REL_TOL) != (xr < ro.REL_TOL)
+    record(tag, "ionised flag", "disagreeing cells / N^3", dis.mean(), "<= 1e-4, near-threshold only")
+    assert dis.mean() <= 1e-4 and np.all(near[dis])
+    part = ~near & (xr >= ro.REL_TOL)
+    e = float(np.max(np.abs(res["xH"][part] - xr[part])))
+    record(tag, "xH (partial cells)", "max |gpu - reference|", e, "<= 1e-4")
+    assert e <= 1e-4
+    zd = int((res["z_at_ionization"][~near] != ref["z_at_ionization"].reshape(n, n, n)[~near]).sum())
+    record(tag, "z_at_ionization", "differing cells outside near-threshold", zd, "= 0")
+    assert zd == 0
+    e = rel_l2(res["temp_kinetic_all_gas"][~near], ref["temp_kinetic_all_gas"].reshape(n, n, n)[~near])
+    record(tag, "temp_kinetic_all_gas", "relative L2", e, "<= 1e-5")
+    assert e <= 1e-5
+    dxh = abs(out.volume_weighted_global_xH - ref["scalars"]["volume_weighted_global_xH"])
+    record(tag, "<xH>", "|gpu - reference|", dxh, "<= 1e-4")
+    assert dxh <= 1e-4
+
+
+def test_step_chain_against_reference_code():
+    """ComputeTs -> find_HII_bubbles -> delta_T at 32^3 on the GPU against the reference's compiled
+    _ComputeTs, _find_HII_bubbles and ComputeBrightnessTemperatureBox."""
+    ref_lib = _ref_lib()
+    n, box, z = 32, 64.0, 13.0
+    zz, snap = wl.snapshot_redshifts(z)
+    src = wl.make_sources(n, box, 600)
+    ti = wl.make_ts_inputs(src, zz, snap, snap + 1, 601)
+    p = rg.make_params(n, box, Flag_IncludeSpinTemp=1, Flag_EvolvingReionRBubbleMax=0, ReionRBubbleMax=50.0,
+                       ReionEfficiency=3000.0)
+    res, ts, hii, tb = gpu_step(p, zz, snap, src, ti)
+    inputs = dict(deltax=src.deltax, stars=src.stars, weighted_sfr=src.sfr, sfr=src.sfr, xray_luminosity=src.xray,
+                  x_e_box_prev=ti.x_e_box_prev, Tk_box=ti.Tk_box, sfr_histories=np.stack(ti.sfr_histories),
+                  xray_luminosity_histories=np.stack(ti.xray_histories))
+    ref = ref_lib.run_step(oracle_params(p), zz, snap, inputs, stages=("ts", "hii", "dT"),
+                           n_hist=len(ti.sfr_histories), stored_fcoll=ti.stored_fcoll,
+                           outputs=("x_e_box", "Tk_box", "TS_box", "xH", "delta_T"))
+    tag = "chain 32^3 vs reference code"
+    U = wl.from_padded
+    e = rel_l2(U(res["x_e_box"]), U(ref["x_e_box"].reshape(n, n, -1)))
+    record(tag, "x_e_box", "relative L2", e, "<= 1e-5")
+    assert e <= 1e-5
+    for k in ("Tk_box", "TS_box"):
+        e = rel_l2(res[k], ref[k].reshape(n, n, n))
+        record(tag, k, "relative L2", e, "<= 1e-5")
+        assert e <= 1e-5, k
+    e = abs(tb / ref["scalars"]["volume_ave_Tb"] - 1.0)
+    record(tag, "<T_b>", "relative", e, "<= 1e-4")
+    assert e <= 1e-4
+    dxh = abs(hii.volume_weighted_global_xH - ref["scalars"]["volume_weighted_global_xH"])
+    record(tag, "<xH>", "|gpu - reference|", dxh, "<= 1e-4")
+    assert dxh <= 1e-4
