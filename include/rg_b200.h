@@ -305,6 +305,16 @@ int rg_profile_read(rg_context* ctx, rg_kernel_stat* out, int max, int* n);
 int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* d_in_padded,
                               float* d_out_padded, double R, int filter_type);
 
+/* Bounds of the device waits, for tests of their time-out paths (no counterpart in the
+   reference, whose CPU loops have no waits).  xy_poll_limit: checks a Y item of the fused x/y
+   pass makes for its plane's X items before it gives up (default 2^22, sleeping 64 ns between
+   checks); xy_signal = 0 stops X items from signalling, so every Y wait runs out; the pass then
+   completes with unordered planes and the call returns RG_ETIMEDOUT.  ts_iteration_limit:
+   get_Ts fixed-point iterations per cell (default 10000); a cell that reaches it makes
+   rg_compute_Ts return RG_ETIMEDOUT.  A negative (poll) or non-positive (iteration) value
+   restores the default; larger values are cut to the defaults. */
+int rg_debug_set_wait_limits(rg_context* ctx, int xy_poll_limit, int xy_signal, int ts_iteration_limit);
+
 /* Radius schedule of find_HII_bubbles: fills up to max_r radii, returns the count in *n. */
 int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int max_r, int* n);
 

@@ -370,6 +370,14 @@ int rg_set_radius_batch(rg_context* ctx, int k) {
   return RG_OK;
 }
 
+int rg_debug_set_wait_limits(rg_context* ctx, int xy_poll_limit, int xy_signal, int ts_iteration_limit) {
+  if (!ctx) return RG_EINVAL;
+  ctx->xy_poll_limit = xy_poll_limit < 0 ? RG_XY_POLL_LIMIT : std::min(xy_poll_limit, RG_XY_POLL_LIMIT);
+  ctx->xy_signal = xy_signal != 0;
+  ctx->ts_iter_limit = ts_iteration_limit < 1 ? RG_TS_ITER_LIMIT : std::min(ts_iteration_limit, RG_TS_ITER_LIMIT);
+  return RG_OK;
+}
+
 int rg_set_stream(rg_context* ctx, void* stream) {
   if (!ctx) return RG_EINVAL;
   ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;

@@ -51,6 +51,9 @@ constexpr int RECFAST_NPTS = 501;
 constexpr int KAPPA_10_NPTS = 27;
 constexpr int KAPPA_10_elec_NPTS = 20;
 constexpr int KAPPA_10_pH_NPTS = 17;
+// default bounds of the device waits
+#define RG_XY_POLL_LIMIT (1 << 22)
+#define RG_TS_ITER_LIMIT 10000
 
 struct cf;
 
@@ -230,6 +233,11 @@ struct rg_context {
   // fused x/y pass control words: [0] error word, [1] item counter, [2 ..) per-job counts
   uint32_t* xy_ctrl = nullptr;
   size_t xy_ctrl_elems = 0;
+  // bounds of the device waits (rg_debug_set_wait_limits): polls of a fused-pass Y item for its
+  // plane's X items, whether X items signal at all, and get_Ts fixed-point iterations per cell
+  int xy_poll_limit = RG_XY_POLL_LIMIT;
+  int xy_signal = 1;
+  int ts_iter_limit = RG_TS_ITER_LIMIT;
   int num_sms = 0;
   // host entry points: uploads and early downloads run on copy_stream, ordered by these events
   cudaStream_t copy_stream = nullptr;

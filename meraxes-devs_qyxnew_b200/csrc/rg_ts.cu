@@ -26,6 +26,7 @@
 #include "rg_internal.h"
 #include "rg_pass.cuh"
 #include "rg_xray.h"
+#include "rg_xyf.cuh"
 
 namespace rg {
 
@@ -55,6 +56,8 @@ struct TsZConst {
 struct TsDev {
   KappaSpline k10, kel, kpH;
   TsZConst z;
+  int max_iter;   // get_Ts fixed-point iterations before a cell counts as not converged
+  int pad_;
 };
 
 __device__ __forceinline__ double spline_eval(const KappaSpline& s, double x) {
@@ -89,8 +92,9 @@ __device__ __forceinline__ double log_kappa_table(const KappaSpline& s, double l
 
 // get_Ts with xcoll and the Wouthuysen-Field coupling (XRayHeatingFunctions.c:1639-1726,
 // 1973-2008).  The factors that do not change across the fixed-point iterations (xcoll, the
-// S_alpha terms in T_K only, xi) are evaluated once per cell.  The loop is capped at 10000
-// iterations; a cell that reaches the cap counts in *nonconv.
+// S_alpha terms in T_K only, xi) are evaluated once per cell.  The loop is capped at
+// C.max_iter iterations (10000 unless a test lowers it); a cell that reaches the cap counts in
+// *nonconv.
 __device__ float get_Ts(const TsDev& C, float delta, float TK, float xe, float Jalpha, float* curr_xalpha,
                         int* nonconv) {
   const TsZConst& Z = C.z;
@@ -113,7 +117,7 @@ __device__ float get_Ts(const TsDev& C, float delta, float TK, float xe, float J
     double TSold = 0.0, xa_tilde = 0.0;
     int it = 0;
     while (fabs(TS - TSold) / TS > 1.0e-3) {
-      if (++it > 10000) {
+      if (++it > C.max_iter) {
         *nonconv += 1;
         break;
       }
@@ -647,15 +651,44 @@ static void fill_spline(const CubicSpline& sp, const std::vector<double>& lx, co
   }
 }
 
-// x and y passes of a batch of shells: work_base + (j * bt.ng + g) * stride, j < bt.nr
+// the batch of shells as the fused x/y pass's operation: grid g of shell r is the combination
+// sum_i cs[r][i] spec[ks[r][i]][g], windowed by row wrow[r] (or the sharp-k step), into
+// work + (r G + g) stride
+struct TsXOp {
+  const cf* spec;
+  size_t stride;
+  cf* work;
+  TsBatch bt;
+  const float* wtab;
+  int wpitch;
+  const int* wcut;
+  __device__ int grids() const { return bt.ng; }
+  __device__ int nsrc(int r) const { return bt.nk[r]; }
+  __device__ const cf* src(int r, int g, int i) const { return spec + ((size_t)bt.ks[r][i] * bt.ng + g) * stride; }
+  __device__ float coef(int r, int i) const { return bt.cs[r][i]; }
+  __device__ bool filtered(int r) const { return bt.filtered[r] != 0; }
+  __device__ const float* wrow(int r) const { return wtab + (size_t)bt.wrow[r] * wpitch; }
+  __device__ int cutoff(int r) const { return wcut ? __ldg(wcut + bt.wrow[r]) : -2; }
+  __device__ cf* out(int r, int g) const { return work + ((size_t)r * bt.ng + g) * stride; }
+};
+
+// x and y passes of a batch of shells: work_base + (j * bt.ng + g) * stride, j < bt.nr.  Fused
+// mode runs them as one kernel (the y pass reads each plane from L2); plain mode as two.
 template <int N>
 static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
                         const float* wtab, int wpitch, const int* wcut, cudaStream_t st) {
+  using C = Cfg<N>;
+  const double nzc = (double)C::NZ * N * N;
+  if (ctx->mode == RG_MODE_FUSED) {
+    double src_reads = 0;
+    for (int r = 0; r < bt.nr; ++r) src_reads += bt.nk[r];
+    const TsXOp op{spec, stride, work_base, bt, wtab, wpitch, wcut};
+    return launch_xy_fused<N>(ctx, op, bt.nr, "ts_xy_c2c_combine_window", bt.ng * 8.0 * nzc * (src_reads + bt.nr),
+                              st);
+  }
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
-  using C = Cfg<N>;
-  const double nzc = (double)C::NZ * N * N;
   const size_t smx = sizeof(cf) * (N + (size_t)line_buf<N, C::BX>());
   RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_x<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx));
   prof_begin(ctx, "ts_x_c2c_combine_window", st);
@@ -761,6 +794,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   fill_spline(ctx->tables.k10, ctx->tables.k10_lT, ctx->tables.k10_lk, &hc.k10);
   fill_spline(ctx->tables.kel, ctx->tables.kel_lT, ctx->tables.kel_lk, &hc.kel);
   fill_spline(ctx->tables.kpH, ctx->tables.kpH_lT, ctx->tables.kpH_lk, &hc.kpH);
+  hc.max_iter = ctx->ts_iter_limit;
   {
     // per-redshift factors of xcoll / taugp / xalpha_tilde / dT_comp / evolveInt; the C passes
     // the redshift to them as a float
@@ -800,6 +834,7 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double Mh2 = rtom(p, R0) * p->Hubble_h * p->Hubble_h;
   const double ftpr3 = (4.0 / 3.0) * M_PI * std::pow(R0, 3.0) / pixel_volume;
 
+  bool xy_used = false;   // the fused x/y pass ran: its error word is read at the end
   auto finish = [&](bool homog, int nblocks) -> int {
     if ((rc = kick())) return rc;
     if ((rc = reduce_partials(ctx, partials, nblocks, TS_NSUM, ctx->d_sums, st))) return rc;
@@ -822,7 +857,10 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     out->volume_ave_TK = S[5] / nn;
     out->volume_ave_xe = S[6] / nn;
     out->homogeneous = homog;
-    if (nonconv) return set_error(ctx, RG_ETIMEDOUT, "get_Ts did not converge in 10000 iterations for some cells");
+    if (nonconv)
+      return set_error(ctx, RG_ETIMEDOUT, "get_Ts did not converge in " + std::to_string(ctx->ts_iter_limit) +
+                                              " iterations for some cells");
+    if (xy_used) return xy_ctrl_check(ctx, st);
     return RG_OK;
   };
 
@@ -912,6 +950,10 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
                            ctx->wcut)))
       return rc;
     const int* wcut = p->TsHeatingFilterType == 1 ? ctx->wcut : nullptr;
+    if (ctx->mode == RG_MODE_FUSED) {
+      if ((rc = xy_ctrl_reset(ctx, (size_t)(N / 2 + 1) * TS_KB, st))) return rc;
+      xy_used = true;
+    }
 
     // Batches of TS_KB shells: the forward transforms of the sources a batch uses first (`used`
     // is in order of first use), then its x and y passes into work[r][g].  From host arrays,

@@ -38,6 +38,8 @@ struct XYSched {
   uint32_t* ctr;     // item counter (zero at launch)
   uint32_t* done;    // [J] finished X items per job (zero at launch)
   uint32_t* err;     // set to 1 when a wait runs out
+  int max_polls;     // polls of a Y item's wait before it gives up
+  int signal;        // X items signal their job (0 only in the forced-timeout test)
 };
 
 __device__ __forceinline__ void xy_decode(const XYSched& s, int seg, bool& is_y, int& job) {
@@ -63,10 +65,11 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
   return v;
 }
 
-// thread 0 only: wait until job's X items have all signalled (at most ~2^22 polls)
+// thread 0 only: wait until job's X items have all signalled (at most max_polls + 1 checks)
 __device__ __forceinline__ void xy_wait(const XYSched& s, int job) {
-  for (int i = 0; i < (1 << 22); ++i) {
+  for (int i = 0;; ++i) {
     if (ld_acquire_u32(s.done + job) >= (uint32_t)s.M) return;
+    if (i >= s.max_polls) break;
     __nanosleep(64);
   }
   atomicExch(s.err, 1u);
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
             [&](int p) { return line_addr<N, B>(p, b); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
       }
       __syncthreads();   // every store of the item is issued
-      if (threadIdx.x == 0) xy_signal(sch.done + job);
+      if (threadIdx.x == 0 && sch.signal) xy_signal(sch.done + job);
     } else {
       if (threadIdx.x == 0) xy_wait(sch, job);
       __syncthreads();
@@ -209,6 +212,8 @@ int launch_xy_fused(rg_context* ctx, const Op& op, int nr, const char* name, dou
   s.L = std::min(J, (grid + 2 * F::M - 1) / (2 * F::M) + 1);
   s.total = 2 * J * F::M;
   s.err = ctx->xy_ctrl;
+  s.max_polls = ctx->xy_poll_limit;
+  s.signal = ctx->xy_signal;
   s.ctr = ctx->xy_ctrl + 1;
   s.done = ctx->xy_ctrl + 2;
   RG_CUDA_TRY(ctx, cudaMemsetAsync(s.ctr, 0, sizeof(uint32_t) * ((size_t)J + 1), st));

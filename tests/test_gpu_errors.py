@@ -1,6 +1,8 @@
 """Status codes of the C ABI on a GPU: invalid arguments and unimplemented configurations return
 RG_EINVAL / RG_EUNSUPPORTED with a message (the reference aborts the run instead), nothing is
-launched for them, and the context stays usable afterwards."""
+launched for them, and the context stays usable afterwards.  The two bounded device waits (the
+fused pass's wait for a plane's x pass, get_Ts's fixed point) are made to run out through
+rg_debug_set_wait_limits: the calls return RG_ETIMEDOUT and the context keeps working."""
 
 import ctypes as C
 
@@ -105,3 +107,84 @@ def test_delta_T_and_power_spectrum_rejections():
     kk, ps, err = ctx.power_spectrum(p, d.data_ptr())
     assert len(kk) == nb.value
     ctx.close()
+
+
+def _hii_case(n, box):
+    src = wl.make_sources(n, box, seed=11)
+    dg = DeviceGrids(n)
+    dg.put("deltax", src.deltax)
+    dg.put("stars", src.stars)
+    dg.put("weighted_sfr", src.sfr)
+    zz, snap = wl.snapshot_redshifts(8.0)
+    p = rg.make_params(n, box, Flag_EvolvingReionRBubbleMax=0, ReionRBubbleMax=30.0, ReionEfficiency=3000.0)
+    return dg, p, rg.snapshot(zz, snap)
+
+
+def test_fused_pass_wait_time_out_is_reported_and_context_survives():
+    """The fused x/y pass's only cross-block wait, made to run out: X items do not signal (a flag
+    that nothing sets), each Y item gives up after 16 checks, the kernel completes and the call
+    returns RG_ETIMEDOUT.  Restored limits give the same result as a fresh context, bit for bit."""
+    n, box = 64, 64.0
+    dg, p, s = _hii_case(n, box)
+    ctx = rg.Context(n)
+    out = rg.rg_hii_scalars()
+    assert status(ctx, "rg_debug_set_wait_limits", 16, 0, -1) == rg.RG_OK
+    rc = status(ctx, "rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out))
+    assert rc == rg.RG_ETIMEDOUT
+    assert "wait" in ctx.lib.rg_last_error(ctx.h).decode()
+    assert status(ctx, "rg_debug_set_wait_limits", -1, 1, -1) == rg.RG_OK
+    dg.t["z_at_ionization"].fill_(-1.0)
+    dg.t["J_21_at_ionization"].zero_()
+    dg.t["temp_kinetic_all_gas"].zero_()
+    assert status(ctx, "rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out)) == rg.RG_OK
+    got = {k: dg.get(k).copy() for k in ("xH", "z_at_ionization", "J_21_at_ionization", "temp_kinetic_all_gas")}
+    ctx.close()
+    fresh, _, _ = _hii_case(n, box)
+    ctx2 = rg.Context(n)
+    out2 = rg.rg_hii_scalars()
+    assert status(ctx2, "rg_find_HII_bubbles", C.byref(p), C.byref(s), C.byref(fresh.g), C.byref(out2)) == rg.RG_OK
+    ctx2.close()
+    for k, v in got.items():
+        assert np.array_equal(v, fresh.get(k)), k
+    assert out.volume_weighted_global_xH == out2.volume_weighted_global_xH
+
+
+def test_get_ts_iteration_cap_is_reported_and_context_survives():
+    """get_Ts capped at one fixed-point iteration: cells that need more make rg_compute_Ts return
+    RG_ETIMEDOUT; with the default cap restored the same context gives the fresh-context result."""
+    import torch
+    n, box = 32, 64.0
+    zz, idx = wl.snapshot_redshifts(15.0)
+    src = wl.make_sources(n, box, 400)
+    ti = wl.make_ts_inputs(src, zz, idx, idx + 1, 401)
+    p = rg.make_params(n, box, Flag_IncludeSpinTemp=1)
+
+    def run(ctx):
+        dg = DeviceGrids(n, spin=True)
+        for k, v in (("deltax", src.deltax), ("stars", src.stars), ("sfr", src.sfr), ("xray_luminosity", src.xray),
+                     ("x_e_box_prev", ti.x_e_box_prev), ("Tk_box", ti.Tk_box)):
+            dg.put(k, v)
+        hs = torch.from_numpy(np.stack(ti.sfr_histories).ravel()).cuda()
+        hx = torch.from_numpy(np.stack(ti.xray_histories).ravel()).cuda()
+        dg.g.sfr_histories, dg.g.xray_luminosity_histories = hs.data_ptr(), hx.data_ptr()
+        dg.g.n_hist = len(ti.sfr_histories)
+        s = rg.snapshot(zz, idx, ti.stored_fcoll.copy())
+        out = rg.rg_ts_scalars()
+        rc = status(ctx, "rg_compute_Ts", C.byref(p), C.byref(s), C.byref(dg.g), C.byref(out))
+        return rc, {k: dg.get(k).copy() for k in ("x_e_box", "Tk_box", "TS_box")}
+
+    ctx = rg.Context(n)
+    assert status(ctx, "rg_debug_set_wait_limits", -1, 1, 1) == rg.RG_OK
+    rc, _ = run(ctx)
+    assert rc == rg.RG_ETIMEDOUT
+    assert "get_Ts" in ctx.lib.rg_last_error(ctx.h).decode()
+    assert status(ctx, "rg_debug_set_wait_limits", -1, 1, -1) == rg.RG_OK
+    rc, got = run(ctx)
+    assert rc == rg.RG_OK
+    ctx.close()
+    ctx2 = rg.Context(n)
+    rc2, want = run(ctx2)
+    ctx2.close()
+    assert rc2 == rg.RG_OK
+    for k in got:
+        assert np.array_equal(got[k], want[k]), k
