@@ -8,7 +8,7 @@
 //   z pass : per block of rows, for each radius of the batch in order: c2r of the G grids into
 //            shared memory, then the aliasing clamp and the barrier test per cell.
 // Until the last radius the per-cell state is two bits (ionized this snapshot; z_at_ionization
-// still < 0), kept in registers within a batch and in a packed word array between batches;
+// still < 0), kept in registers within a batch and in one byte per cell between batches;
 // z_at_ionization and J_21 are written only where a cell first ionizes.  The last radius also
 // computes the partial xH and runs the closing pass (temperatures and FP64 global sums).
 #include <cuda_runtime.h>
@@ -17,10 +17,13 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "rg_internal.h"
 #include "rg_pass.cuh"
+#include "rg_tma.cuh"
 #include "rg_xyf.cuh"
 
 namespace rg {
@@ -58,6 +61,7 @@ __global__ void k_window_table(float* wtab, int n2max, const double* __restrict_
     if (ftype == 1 && wcut && w == 1.0 && (n2 == n2max || sharpk_zero(delta_k, n2 + 1, R))) wcut[r] = n2;
   }
 }
+
 
 // ---------------------------------------------------------------------------
 // inverse x pass with the window and a batch of radii: grid g of spec (spec + g * stride) is
@@ -198,7 +202,8 @@ struct HiiState {
   const float* wsfrIII;      // padded, Pop III only
   float* Gamma12;            // recombination branch: written at a cell's first crossing
   float* r_bubble;
-  uint32_t* bits;            // [2][nblocks][W][NTH]
+  uint8_t* st8;              // per cell between radius batches: bit 0 = z_at_ionization still < 0,
+                             // bit 1 = ionised at a radius of this snapshot
   double* partials;          // [nblocks][HII_NSUM]
 };
 
@@ -246,29 +251,30 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
   cf* tiles = reinterpret_cast<cf*>(rt + round_up((EXT ? bt.ng : NG) * ROWS * RP, 4));
   const int x = blockIdx.y, y0 = blockIdx.x * ROWS;
   const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
-  const size_t nwords = (size_t)gridDim.x * gridDim.y * W * NTH;
   load_twiddles<N>(s_tw, g_tw);
 
   // per-cell state bits: A = z_at_ionization still < 0, I = ionized at a radius of this snapshot.
-  // Cell it of this thread is block cell threadIdx.x + it * NTH, bit it % 32 of word it / 32.
+  // Cell it of this thread is block cell threadIdx.x + it * NTH, bit it % 32 of word it / 32;
+  // between batches the state is one byte per cell (s.st8, bit 0 = A, bit 1 = I).
   uint32_t A[W], I[W];
 #pragma unroll
   for (int w = 0; w < W; ++w) {
-    if (bt.first) {
-      uint32_t a = 0u;
-      const int nb = IT - 32 * w < 32 ? IT - 32 * w : 32;
+    uint32_t a = 0u, iv = 0u;
+    const int nb = IT - 32 * w < 32 ? IT - 32 * w : 32;
 #pragma unroll 8
-      for (int bb = 0; bb < nb; ++bb) {
-        const int i = threadIdx.x + (32 * w + bb) * NTH;
-        const size_t ir = ((size_t)x * N + y0 + i / N) * N + i % N;
+    for (int bb = 0; bb < nb; ++bb) {
+      const int i = threadIdx.x + (32 * w + bb) * NTH;
+      const size_t ir = ((size_t)x * N + y0 + i / N) * N + i % N;
+      if (bt.first) {
         if (s.z_in[ir] < 0.f) a |= 1u << bb;
+      } else {
+        const uint32_t v = s.st8[ir];
+        a |= (v & 1u) << bb;
+        iv |= ((v >> 1) & 1u) << bb;
       }
-      A[w] = a;
-      I[w] = 0u;
-    } else {
-      A[w] = s.bits[(blk * W + w) * NTH + threadIdx.x];
-      I[w] = s.bits[nwords + (blk * W + w) * NTH + threadIdx.x];
     }
+    A[w] = a;
+    I[w] = iv;
   }
   // the Pop III and recombination grids (only the 9-grid instantiation runs with them, so the
   // others compile without those branches)
@@ -461,8 +467,13 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QZ, (HiiZ<N, FINAL>::MINB))
   if constexpr (!FINAL) {
 #pragma unroll
     for (int w = 0; w < W; ++w) {
-      s.bits[(blk * W + w) * NTH + threadIdx.x] = A[w];
-      s.bits[nwords + (blk * W + w) * NTH + threadIdx.x] = I[w];
+      const int nb = IT - 32 * w < 32 ? IT - 32 * w : 32;
+#pragma unroll 8
+      for (int bb = 0; bb < nb; ++bb) {
+        const int i = threadIdx.x + (32 * w + bb) * NTH;
+        const size_t ir = ((size_t)x * N + y0 + i / N) * N + i % N;
+        s.st8[ir] = (uint8_t)(((A[w] >> bb) & 1u) | (((I[w] >> bb) & 1u) << 1));
+      }
     }
   } else {
     block_sum<NTH, HII_NSUM>(acc, s.partials + blk * HII_NSUM);
@@ -656,6 +667,192 @@ int launch_forward(rg_context* ctx, const float* const* d_real, int ng, cf* spec
   return RG_OK;
 }
 
+
+// f(std::integral_constant<int, I>{}) for I in the sequence, in order
+template <class F, int... I>
+__device__ __forceinline__ void for_each_index(std::integer_sequence<int, I...>, F&& f) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+
+// ---------------------------------------------------------------------------
+// z pass of a batch before the last one (no recombination or Pop III grid), with the tiles staged
+// by TMA and the barrier test on the transforms' registers.
+//
+// The block owns rows [y0, y0 + 2Q) of plane x.  For every (radius, grid) unit u of the batch, the
+// Hermitian half column tile (all kz, those rows) arrives in shared memory by tensor loads (ZB
+// tiles in flight, one mbarrier each); the c2r of its row pairs leaves each thread the same cells
+// of every grid (the transform's output positions do not depend on the grid), so the previous
+// grids' values are kept in registers and the clamp and barrier test run as the last grid's
+// values come out of the transform: no row buffer in shared memory.  The state of a cell
+// (z_at_ionization still < 0; ionised at a radius of this snapshot) is two bits in registers
+// within the batch and one byte per cell between batches.
+template <int N>
+struct HiiZR {
+  static constexpr int T = Cfg<N>::T, Q = Cfg<N>::QZ, NTH = T * Q, V = N / T;
+  static constexpr int NZ = N / 2 + 1;
+  // kz rows per tensor box (box dimensions are at most 256): one box, or for N = 512 two boxes of
+  // (NZ + 1) / 2 rows at kz 0 and kz NZ - KZB that overlap in one row, so the second box lands on
+  // a 128-byte boundary of the tile and no row lies outside the tensor
+  static constexpr int KZB = NZ <= 256 ? NZ : (NZ + 1) / 2;
+  static constexpr int NBOX = NZ <= 256 ? 1 : 2;
+  static constexpr int TB = round_up(cmax(NZ * 2 * Q, line_buf<N, Q>()), 16);   // 128-byte multiple
+  static constexpr int ZB = 3;                                 // tiles in flight
+  static constexpr uint32_t TX = (uint32_t)(NBOX * KZB * 2 * Q * sizeof(cf));   // bytes the boxes deliver
+  static_assert(NBOX == 1 || ((NZ - KZB) * 2 * Q * sizeof(cf)) % 128 == 0, "second box off a 128-byte boundary");
+  static constexpr size_t smem() { return 128 + sizeof(cf) * ((size_t)ZB * TB + N) + sizeof(uint64_t) * ZB; }
+  // resident blocks: register room for the kept grids (up to 3 x 2V floats) without spills
+  static constexpr int MINB = NTH >= 256 ? 2 : 3;
+  // the sizes it serves: power-of-two grids of 64^3 and up (at most 16 values per thread)
+  static constexpr bool USED = (N == 64 || N == 128 || N == 256 || N == 512);
+  static_assert(2 * V <= 64, "two state bits per cell in 64-bit masks");
+};
+
+constexpr int TMA_WAIT_LIMIT = 1 << 22;   // polls of an mbarrier before a wait gives up
+
+template <int N, bool SPIN, bool BH>
+__global__ void __launch_bounds__(HiiZR<N>::NTH, HiiZR<N>::MINB)
+    k_hii_zr(const __grid_constant__ CUtensorMap tmap, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
+             HiiState s, uint32_t* err) {
+  using Z = HiiZR<N>;
+  using PL = Plan<N>;
+  constexpr int Q = Z::Q, V = Z::V, ZB = Z::ZB, TB = Z::TB, NZ = Z::NZ, KZB = Z::KZB, NBOX = Z::NBOX;
+  constexpr int NG = 2 + SPIN + BH;          // deltax, stars, [x_e], [effective_bhm]
+  constexpr int GX = 2, GB = 2 + SPIN;       // grid indices of x_e and effective_bhm
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* sm = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  cf* tiles = reinterpret_cast<cf*>(sm);
+  cf* s_tw = tiles + ZB * TB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
+  const int x = blockIdx.y, y0 = blockIdx.x * 2 * Q;
+  const int q = threadIdx.x % Q, tq = threadIdx.x / Q;
+  const int nunits = bt.nr * NG;
+
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < ZB; ++b) mbar_init(&bars[b], 1);
+    mbar_init_fence();
+  }
+  load_twiddles<N>(s_tw, g_tw);
+  __syncthreads();
+  // thread 0: tensor loads of unit u into tile u % ZB (tensor coordinates: y in floats, x, kz of
+  // the unit's spectrum stacked after the previous units)
+  auto issue = [&](int u) {
+    const int b = u % ZB;
+    mbar_arrive_expect_tx(&bars[b], Z::TX);
+#pragma unroll
+    for (int k = 0; k < NBOX; ++k) {
+      const int k0 = k ? NZ - KZB : 0;
+      tma_load_3d(tiles + b * TB + k0 * 2 * Q, &tmap, 2 * y0, x, u * NZ + k0, &bars[b]);
+    }
+  };
+  if (threadIdx.x == 0)
+    for (int u = 0; u < ZB && u < nunits; ++u) issue(u);
+
+  // state of this thread's 2V cells: cell 2 slot + h is row y0 + 2q + h at z = last_pos(tq, slot)
+  uint64_t A = 0, I = 0;
+#pragma unroll
+  for (int slot = 0; slot < V; ++slot) {
+    const int z = last_pos<PL>(tq, slot);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
+      const uint64_t bit = 1ull << (2 * slot + h);
+      if (bt.first) {
+        if (s.z_in[ir] < 0.f) A |= bit;
+      } else {
+        const uint32_t v = s.st8[ir];
+        if (v & 1u) A |= bit;
+        if (v & 2u) I |= bit;
+      }
+    }
+  }
+
+  float vals[NG - 1][2 * V];   // the transformed grids before the last one, for the radius in work
+  bool waited = true;
+  int u = 0;
+  for (int r = 0; r < bt.nr; ++r) {
+    const double pref = bt.fcoll_pref[r];
+    const float jaux = bt.J_aux[r], jaux_bh = bt.J_aux_bh[r];
+    // one (radius, grid) unit; the grid index is a compile-time constant (register arrays)
+    auto unit = [&](auto gconst) {
+      constexpr int g = decltype(gconst)::value;
+      const int b = u % ZB;
+      cf* tile = tiles + b * TB;
+      if (!mbar_wait(&bars[b], (uint32_t)((u / ZB) & 1), TMA_WAIT_LIMIT)) waited = false;
+      line_fft_p<PL, true>(
+          tq, tile, s_tw, [&](int p, int) { return ztile_c2r_input<N, Q>(tile, q, p); },
+          [&](int p) { return line_addr<N, Q>(p, q); },
+          [&](int z, cf v, int slot) {
+            if constexpr (g < NG - 1) {
+              vals[g][2 * slot] = v.x;
+              vals[g][2 * slot + 1] = v.y;
+            } else {
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const float last = h ? v.y : v.x;
+                auto val = [&](auto gi) -> float {
+                  constexpr int gg = decltype(gi)::value;
+                  if constexpr (gg == NG - 1) return last;
+                  else return vals[gg][2 * slot + h];
+                };
+                // the aliasing clamp (find_HII_bubbles.c:373-422) and the barrier test of
+                // k_hii_z without recombinations or Pop III
+                const float dx = fmaxf(val(std::integral_constant<int, 0>{}), -1.f + REL_TOL);
+                float st = fmaxf(val(std::integral_constant<int, 1>{}), 0.f);
+                if (st < ABS_TOL) st = 0.f;
+                float xe = 0.f, bhm = 0.f;
+                if constexpr (SPIN) {
+                  xe = fmaxf(val(std::integral_constant<int, GX>{}), 0.f);
+                  if (xe < ABS_TOL) xe = 0.f;
+                  xe = fminf(xe, 0.999f);
+                }
+                if constexpr (BH) {
+                  bhm = fmaxf(val(std::integral_constant<int, GB>{}), 0.f);
+                  if (bhm < ABS_TOL) bhm = 0.f;
+                }
+                const double dom = 1.0 + (double)dx;
+                const double nf = SPIN ? 1.0 - (double)xe : 1.0;
+                const double num = BH ? (double)bhm + (double)st : (double)st;
+                const bool ion = num * pref > nf * (1.0 + 0.0) * dom;
+                const uint64_t bit = 1ull << (2 * slot + h);
+                if (ion) {
+                  I |= bit;
+                  if (A & bit) {
+                    // new ionization (find_HII_bubbles.c:531-543)
+                    A &= ~bit;
+                    const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
+                    s.z_in[ir] = c.redshift;
+                    if (c.uvb == 1) {
+                      float j = st * jaux;
+                      if (BH) j += bhm * jaux_bh;
+                      s.J21[ir] = j;
+                    }
+                  }
+                }
+              }
+            }
+          });
+      // every thread is done with tile b (read by the first stage, exchange buffer after that):
+      // order those generic accesses before the tensor load that refills it
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0 && u + ZB < nunits) issue(u + ZB);
+      ++u;
+    };
+    for_each_index(std::make_integer_sequence<int, NG>{}, unit);
+  }
+  if (!waited && threadIdx.x % 32 == 0) atomicExch(err, 1u);
+#pragma unroll
+  for (int slot = 0; slot < V; ++slot) {
+    const int z = last_pos<PL>(tq, slot);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
+      const int sh = 2 * slot + h;
+      s.st8[ir] = (uint8_t)(((A >> sh) & 1ull) | (((I >> sh) & 1ull) << 1));
+    }
+  }
+}
+
 // the batch of the fused x/y pass: grid g of spec windowed for radius r into work (r ng + g)
 struct HiiXOp {
   const cf* spec;
@@ -739,9 +936,48 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   return RG_OK;
 }
 
+template <int N, bool SPIN, bool BH>
+int launch_hii_zr3(rg_context* ctx, const cf* work, const HiiBatch& bt, const HiiConst& c, const HiiState& s,
+                   cudaStream_t st, int* nblocks) {
+  using Z = HiiZR<N>;
+  constexpr int NG = 2 + SPIN + BH;
+  const cf* tw;
+  int rc = twiddles_for(ctx, N, &tw);
+  if (rc) return rc;
+  // the batch's units as one 3-D float tensor: y (2N floats), x (N), kz of unit u at u NZ + kz
+  CUtensorMap map;
+  const uint64_t dims[3] = {2ull * N, (uint64_t)N, (uint64_t)Z::NZ * bt.nr * NG};
+  const uint64_t strides[2] = {8ull * N, 8ull * N * N};
+  const uint32_t box[3] = {4u * Z::Q, 1u, (uint32_t)Z::KZB};
+  const int mrc = tma_map_3d(&map, work, dims, strides, box);
+  if (mrc != 0) return set_error(ctx, RG_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(mrc) + ")");
+  auto kern = k_hii_zr<N, SPIN, BH>;
+  RG_CUDA_TRY(ctx, prep(kern, Z::smem()));
+  const dim3 grid(N / (2 * Z::Q), N);
+  const double n3 = (double)N * N * N, nzc = (double)Z::NZ * N * N;
+  // algorithmic bytes: the Hermitian halves of NG grids per radius, the state (z_at_ionization on
+  // the first batch, one byte per cell read otherwise, one written)
+  const double bytes = bt.nr * NG * 8.0 * nzc + (bt.first ? 4.0 * n3 : 1.0 * n3) + 1.0 * n3;
+  prof_begin(ctx, "inv_z_c2r_test", st);
+  kern<<<grid, Z::NTH, Z::smem(), st>>>(map, tw, bt, c, s, ctx->xy_ctrl);
+  prof_end(ctx, bytes, st);
+  RG_CUDA_TRY(ctx, cudaGetLastError());
+  if (nblocks) *nblocks = (int)(grid.x * grid.y);
+  return RG_OK;
+}
+
 template <int N>
 int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
                  const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
+  // batches before the last one without recombinations or Pop III: TMA tiles, registers
+  if constexpr (HiiZR<N>::USED) {
+    if (!fin && !c.rec && !c.mini) {
+      if (c.spin && c.bh) return launch_hii_zr3<N, true, true>(ctx, work, bt, c, s, st, nblocks);
+      if (c.spin) return launch_hii_zr3<N, true, false>(ctx, work, bt, c, s, st, nblocks);
+      if (c.bh) return launch_hii_zr3<N, false, true>(ctx, work, bt, c, s, st, nblocks);
+      return launch_hii_zr3<N, false, false>(ctx, work, bt, c, s, st, nblocks);
+    }
+  }
   // with recombinations or Pop III (up to 9 grids) one instantiation reads the count from the
   // batch
   if (c.rec || c.mini) {
@@ -763,13 +999,6 @@ int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const H
              : launch_hii_z3<N, 4, false>(ctx, work, stride, bt, c, s, st, nblocks);
 }
 
-// words of packed state per bit kind
-template <int N>
-size_t hii_bit_words() {
-  using C = Cfg<N>;
-  constexpr int NTH = C::T * C::QZ, IT = 2 * C::QZ * N / NTH, W = (IT + 31) / 32;
-  return (size_t)(N / (2 * C::QZ)) * N * W * NTH;
-}
 
 template <int N>
 int launch_debug_inverse(rg_context* ctx, const cf* spec, cf* work, const float* wrow, float* out, cudaStream_t st) {
@@ -838,7 +1067,6 @@ static int hii_z(rg_context* ctx, int n, const cf* work, size_t stride, int ng, 
   RG_DISPATCH_N(n, launch_hii_z<NN>(ctx, work, stride, ng, bt, c, s, fin, st, nblocks));
 }
 
-static size_t bit_words(int n) { RG_DISPATCH_N_VAL(n, hii_bit_words<NN>(), (size_t)0); }
 
 static int hii_recomb(rg_context* ctx, int n, const RecTables& tab, const RecConst& c, const RecState& s,
                       double* partials, int nblocks, cudaStream_t st) {
@@ -940,8 +1168,8 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   if (kb > nr) kb = nr;
   if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * ng))) return rc;
   if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * ng * kb))) return rc;
-  const size_t nw = bit_words(N);
-  if ((rc = ensure_device(ctx, &ctx->bits, &ctx->bits_elems, 2 * nw))) return rc;
+  // one state byte per cell between radius batches (in words of four)
+  if ((rc = ensure_device(ctx, &ctx->bits, &ctx->bits_elems, ((size_t)N * N * N + 3) / 4))) return rc;
   if ((rc = stage_wait(ctx, stg->inputs, st))) return rc;
   for (int g0 = 0; g0 < ng; g0 += MAXG)   // at most MAXG grids per forward launch
     if ((rc = fft_forward(ctx, N, srcs + g0, std::min(MAXG, ng - g0), ctx->spec + nc * g0, nc,
@@ -986,7 +1214,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   hs.wsfrIII = mini ? g->weighted_sfrIII : nullptr;
   hs.Gamma12 = g->Gamma12;
   hs.r_bubble = g->r_bubble;
-  hs.bits = ctx->bits;
+  hs.st8 = reinterpret_cast<uint8_t*>(ctx->bits);
   hs.partials = partials;
 
   if ((rc = xy_ctrl_reset(ctx, (size_t)(N / 2 + 1) * kb, st))) return rc;

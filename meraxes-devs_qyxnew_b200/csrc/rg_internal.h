@@ -187,7 +187,7 @@ struct rg_context {
   size_t spec_elems = 0;
   rg::cf* work = nullptr;
   size_t work_elems = 0;
-  uint32_t* bits = nullptr;      // packed per-cell state of the radius batches
+  uint32_t* bits = nullptr;      // per-cell state between radius batches, one byte per cell
   size_t bits_elems = 0;
   float* wtab = nullptr;         // window table [nR][n2max+1]
   size_t wtab_elems = 0;

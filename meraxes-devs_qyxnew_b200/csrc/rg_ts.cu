@@ -26,7 +26,6 @@
 #include "rg_internal.h"
 #include "rg_pass.cuh"
 #include "rg_xray.h"
-#include "rg_xyf.cuh"
 
 namespace rg {
 
@@ -651,41 +650,14 @@ static void fill_spline(const CubicSpline& sp, const std::vector<double>& lx, co
   }
 }
 
-// the batch of shells as the fused x/y pass's operation: grid g of shell r is the combination
-// sum_i cs[r][i] spec[ks[r][i]][g], windowed by row wrow[r] (or the sharp-k step), into
-// work + (r G + g) stride
-struct TsXOp {
-  const cf* spec;
-  size_t stride;
-  cf* work;
-  TsBatch bt;
-  const float* wtab;
-  int wpitch;
-  const int* wcut;
-  __device__ int grids() const { return bt.ng; }
-  __device__ int nsrc(int r) const { return bt.nk[r]; }
-  __device__ const cf* src(int r, int g, int i) const { return spec + ((size_t)bt.ks[r][i] * bt.ng + g) * stride; }
-  __device__ float coef(int r, int i) const { return bt.cs[r][i]; }
-  __device__ bool filtered(int r) const { return bt.filtered[r] != 0; }
-  __device__ const float* wrow(int r) const { return wtab + (size_t)bt.wrow[r] * wpitch; }
-  __device__ int cutoff(int r) const { return wcut ? __ldg(wcut + bt.wrow[r]) : -2; }
-  __device__ cf* out(int r, int g) const { return work + ((size_t)r * bt.ng + g) * stride; }
-};
-
-// x and y passes of a batch of shells: work_base + (j * bt.ng + g) * stride, j < bt.nr.  Fused
-// mode runs them as one kernel (the y pass reads each plane from L2); plain mode as two.
+// x and y passes of a batch of shells: work_base + (j * bt.ng + g) * stride, j < bt.nr.  (The
+// fused x/y kernel of find_HII_bubbles, run on these batches, measured slower at 512^3: 48.8 ms
+// against 43.5 ms for the two passes; the x pass here reads its history spectra mostly from L2.)
 template <int N>
 static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t stride, const TsBatch& bt,
                         const float* wtab, int wpitch, const int* wcut, cudaStream_t st) {
   using C = Cfg<N>;
   const double nzc = (double)C::NZ * N * N;
-  if (ctx->mode == RG_MODE_FUSED) {
-    double src_reads = 0;
-    for (int r = 0; r < bt.nr; ++r) src_reads += bt.nk[r];
-    const TsXOp op{spec, stride, work_base, bt, wtab, wpitch, wcut};
-    return launch_xy_fused<N>(ctx, op, bt.nr, "ts_xy_c2c_combine_window", bt.ng * 8.0 * nzc * (src_reads + bt.nr),
-                              st);
-  }
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
@@ -834,7 +806,6 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
   const double Mh2 = rtom(p, R0) * p->Hubble_h * p->Hubble_h;
   const double ftpr3 = (4.0 / 3.0) * M_PI * std::pow(R0, 3.0) / pixel_volume;
 
-  bool xy_used = false;   // the fused x/y pass ran: its error word is read at the end
   auto finish = [&](bool homog, int nblocks) -> int {
     if ((rc = kick())) return rc;
     if ((rc = reduce_partials(ctx, partials, nblocks, TS_NSUM, ctx->d_sums, st))) return rc;
@@ -860,7 +831,6 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     if (nonconv)
       return set_error(ctx, RG_ETIMEDOUT, "get_Ts did not converge in " + std::to_string(ctx->ts_iter_limit) +
                                               " iterations for some cells");
-    if (xy_used) return xy_ctrl_check(ctx, st);
     return RG_OK;
   };
 
@@ -950,10 +920,6 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
                            ctx->wcut)))
       return rc;
     const int* wcut = p->TsHeatingFilterType == 1 ? ctx->wcut : nullptr;
-    if (ctx->mode == RG_MODE_FUSED) {
-      if ((rc = xy_ctrl_reset(ctx, (size_t)(N / 2 + 1) * TS_KB, st))) return rc;
-      xy_used = true;
-    }
 
     // Batches of TS_KB shells: the forward transforms of the sources a batch uses first (`used`
     // is in order of first use), then its x and y passes into work[r][g].  From host arrays,
