@@ -650,6 +650,59 @@ static void fill_spline(const CubicSpline& sp, const std::vector<double>& lx, co
   }
 }
 
+// The combination of a shell that reads more than TS_MAXSRC history slots:
+// spec[spare][g] = sum_i cs[i] spec[ks[i]][g] for every grid g, accumulated with fmaf in the order
+// of i as the x pass does (1 x value is exact, so the shell's x pass then reads the same numbers).
+// Sources go in chunks of TS_COMB; later chunks continue from the partial sums.
+constexpr int TS_COMB = 32;
+struct TsComb {
+  int n;
+  int first;   // the chunk starts the sums (else it adds to the spare slot)
+  int ks[TS_COMB];
+  float cs[TS_COMB];
+};
+
+__global__ void __launch_bounds__(256) k_ts_combine(cf* __restrict__ spec, size_t stride, int G, TsComb cb,
+                                                    int spare) {
+  const size_t total = stride * (size_t)G;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t g = e / stride, i = e - g * stride;
+    cf* out = spec + ((size_t)spare * G + g) * stride + i;
+    float ax = 0.f, ay = 0.f;
+    if (!cb.first) {
+      ax = out->x;
+      ay = out->y;
+    }
+    for (int k = 0; k < cb.n; ++k) {
+      const cf v = spec[((size_t)cb.ks[k] * G + g) * stride + i];
+      ax = fmaf(cb.cs[k], v.x, ax);
+      ay = fmaf(cb.cs[k], v.y, ay);
+    }
+    *out = cf{ax, ay};
+  }
+}
+
+static int ts_combine(rg_context* ctx, int n, cf* spec, size_t stride, int G, const std::vector<int>& ks,
+                      const std::vector<float>& cs, int spare, cudaStream_t st) {
+  (void)n;
+  const int blocks = 4 * ctx->num_sms;
+  for (size_t i0 = 0; i0 < ks.size(); i0 += TS_COMB) {
+    TsComb cb;
+    std::memset(&cb, 0, sizeof(cb));
+    cb.first = i0 == 0;
+    cb.n = (int)std::min((size_t)TS_COMB, ks.size() - i0);
+    for (int k = 0; k < cb.n; ++k) {
+      cb.ks[k] = ks[i0 + k];
+      cb.cs[k] = cs[i0 + k];
+    }
+    prof_begin(ctx, "ts_combine_sources", st);
+    k_ts_combine<<<blocks, 256, 0, st>>>(spec, stride, G, cb, spare);
+    prof_end(ctx, 8.0 * stride * G * (cb.n + (cb.first ? 1 : 2)), st);
+    RG_CUDA_TRY(ctx, cudaGetLastError());
+  }
+  return RG_OK;
+}
+
 // x and y passes of a batch of shells: work_base + (j * bt.ng + g) * stride, j < bt.nr.  (The
 // fused x/y kernel of find_HII_bubbles, run on these batches, measured slower at 512^3: 48.8 ms
 // against 43.5 ms for the two passes; the x pass here reads its history spectra mostly from L2.)
@@ -885,13 +938,17 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
           slot_of[k] = (int)used.size();
           used.push_back(k);
         }
+    // a shell that combines more than TS_MAXSRC history snapshots gets its combination formed
+    // beforehand (k_ts_combine) into one of TS_KB spare slots after the used sources
+    bool wide = false;
     for (int r = 0; r < nS; ++r) {
       int nk = 0;
       for (int k = 0; k < sh.nsrc; ++k) nk += sh.coef[(size_t)r * sh.nsrc + k] != 0.f;
-      if (nk > TS_MAXSRC) return set_error(ctx, RG_EUNSUPPORTED, "a shell combines more than 4 history snapshots");
+      wide = wide || nk > TS_MAXSRC;
     }
     const int nused = std::max(1, (int)used.size());
-    if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * G * nused))) return rc;
+    const size_t slots = (size_t)nused + (wide ? TS_KB : 0);
+    if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * G * slots))) return rc;
     // every shell's filtered grids stay in HBM until the fused z pass (G nS spectra)
     if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * G * nS))) return rc;
     // source grid `which` (0 sfr, 1 xray, 2 + j AGN band bands[j]) of source k, on the device
@@ -957,14 +1014,26 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
       bt.ng = G;
       for (int j = 0; j < cnt; ++j) {
         const int r = r0 + j;
-        int nk = 0;
+        std::vector<int> ks;
+        std::vector<float> cs;
         for (int k = 0; k < sh.nsrc; ++k) {
           const float c = sh.coef[(size_t)r * sh.nsrc + k];
           if (c != 0.f) {
-            bt.ks[j][nk] = slot_of[k];
-            bt.cs[j][nk] = c;
-            nk++;
+            ks.push_back(slot_of[k]);
+            cs.push_back(c);
           }
+        }
+        if ((int)ks.size() > TS_MAXSRC) {
+          // spare slot nused + j holds sum_i cs[i] spec[ks[i]], accumulated in the x pass's order
+          const int spare = nused + j;
+          if ((rc = ts_combine(ctx, N, ctx->spec, nc, G, ks, cs, spare, st))) return rc;
+          ks.assign(1, spare);
+          cs.assign(1, 1.f);
+        }
+        const int nk = (int)ks.size();
+        for (int i = 0; i < nk; ++i) {
+          bt.ks[j][i] = ks[i];
+          bt.cs[j][i] = cs[i];
         }
         bt.nk[j] = nk;
         bt.filtered[j] = r > 0;  // no filter on the first shell (ComputeTs.c:529)

@@ -173,3 +173,21 @@ def test_compute_ts_invalid_arguments():
     dg = DeviceGrids(48, spin=True)
     assert lib.rg_compute_Ts(ctx.h, C.byref(p), C.byref(snap), C.byref(dg.g), C.byref(out)) == rg.RG_EUNSUPPORTED
     ctx.close()
+
+
+def test_compute_ts_dense_snapshot_list(ts_tables):
+    """400 snapshots before z = 15: the outer shells combine up to 14 history snapshots each
+    (ComputeTs.c:420-458 loops over any number); those beyond four are combined in k-space before
+    the shell's x pass.  Parity with the oracle as for the default list."""
+    n, box = 32, 64.0
+    zz, idx = wl.snapshot_redshifts(15.0, n_before=400)
+    src = wl.make_sources(n, box, 700)
+    p = rg.make_params(n, box, Flag_IncludeSpinTemp=1)
+    _, _, coef = rg.ts_tables(p, zz, idx, idx + 1, 2e-4, 1e-3, np.zeros(len(zz)), with_freq=False)
+    assert (coef != 0).sum(axis=1).max() > 4
+    n_hist = int(np.nonzero(np.any(coef != 0, axis=0))[0].max()) + 1
+    ti = wl.make_ts_inputs(src, zz, idx, n_hist, 701)
+    out, res = run_gpu_ts(p, zz, idx, src, ti)
+    want, wg = run_oracle_ts(p, ts_tables, zz, idx, src, ti)
+    assert out.homogeneous == 0
+    check_parity(out, res, want, wg, n)

@@ -283,3 +283,17 @@ def test_step_chain_matches_reference():
     near = want[3]["min_margin"] <= 1e-4
     assert rel_l2(ref["delta_T"].reshape(n, n, n)[~near], dT[~near]) <= 1e-5
     assert ref["scalars"]["volume_ave_Tb"] == pytest.approx(tb, rel=1e-5)
+
+
+def test_compute_ts_dense_snapshot_list_matches_reference():
+    """400 snapshots before z = 15, so that shells combine up to 14 history snapshots."""
+    n, box = 32, 64.0
+    zz, idx = wl.snapshot_redshifts(15.0, n_before=400)
+    src = wl.make_sources(n, box, 700)
+    p = params(n, box, Flag_IncludeSpinTemp=1)
+    sh, _ = to.shells_and_sources(p, zz, idx, None, None, None, None, want_grids=False)
+    ti = wl.make_ts_inputs(src, zz, idx, sh.max_slot + 1, 701)
+    ref = ref_lib.run_step(p, zz, idx, ts_inputs(src, ti), stages=("ts",), n_hist=len(ti.sfr_histories),
+                           stored_fcoll=ti.stored_fcoll, outputs=TS_OUT)
+    want, g = oracle_ts(p, zz, idx, src, ti)
+    check_ts(n, ref, want, g, idx)
