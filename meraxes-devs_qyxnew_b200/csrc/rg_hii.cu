@@ -864,9 +864,6 @@ struct HiiXOp {
   int unfiltered;
   const int* wcut;   // sharp-k step ends per radius, or null (window rows are read)
   __device__ int grids() const { return ng; }
-  __device__ int nsrc(int) const { return 1; }
-  __device__ const cf* src(int, int g, int) const { return spec + g * stride; }
-  __device__ float coef(int, int) const { return 1.f; }
   __device__ bool filtered(int r) const { return r != unfiltered; }
   __device__ const float* wrow(int r) const { return wrows + (size_t)r * wpitch; }
   __device__ int cutoff(int r) const { return wcut ? __ldg(wcut + r) : -2; }
@@ -882,7 +879,8 @@ int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, cf* work, size_t 
   const double nzc = (double)C::NZ * N * N;
   if (ctx->mode == RG_MODE_FUSED) {
     const HiiXOp op{spec, stride, ng, work, wrows, wpitch, unfiltered, wcut};
-    return launch_xy_fused<N>(ctx, op, nr, "inv_xy_c2c_window", ng * 8.0 * nzc * (1 + nr), st);
+    if (stride != (size_t)C::NZ * N * N) return set_error(ctx, RG_EINVAL, "fused x/y pass: spectra must be contiguous");
+    return launch_xy_fused<N>(ctx, op, spec, ng, nr, "inv_xy_c2c_window", ng * 8.0 * nzc * (1 + nr), st);
   }
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);

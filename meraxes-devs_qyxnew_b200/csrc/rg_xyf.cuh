@@ -20,12 +20,20 @@
 // unfinished item can always finish: the kernel needs no co-resident grid and no cooperative
 // launch.  A wait that runs out sets the error word and the item goes on (the host reports
 // RG_ETIMEDOUT); no wait is unbounded.
+//
+// An X item's input, the spectrum tile (all x, its B columns) of each grid, arrives in shared
+// memory by tensor loads (TMA, mbarrier completion) into two alternating buffers: the load of the
+// next grid's tile, or of the next X item's first tile, is issued before the current tile is
+// transformed, so the loads overlap the transforms.  A buffer is also the FFT exchange buffer
+// of the tile it holds.
 #pragma once
 
 #include <algorithm>
+#include <string>
 
 #include "rg_internal.h"
 #include "rg_pass.cuh"
+#include "rg_tma.cuh"
 
 namespace rg {
 
@@ -82,8 +90,14 @@ struct XYF {
   static constexpr int B = Cfg<N>::BX;   // columns per X item, lines per Y item
   static constexpr int NTH = T * B;
   static constexpr int M = N / B;
-  static constexpr int XBUF = cmax(line_buf<N, B>(), B * Cfg<N>::PITCH_P);
-  static constexpr size_t smem() { return sizeof(cf) * (size_t)(N + XBUF); }
+  static constexpr int XROWS = N <= 256 ? N : N / 2;   // x rows per tensor box (box dimensions <= 256)
+  static constexpr int NXB = N / XROWS;
+  // a buffer: an X tile [x][B columns], then its exchange buffer; or a Y item's exchange buffer
+  static constexpr int TB = round_up(cmax(cmax(line_buf<N, B>(), B * Cfg<N>::PITCH_P), N * B), 16);
+  static constexpr int ZB = 2;
+  static constexpr uint32_t TX = (uint32_t)(N * B * sizeof(cf));
+  static constexpr size_t smem() { return 128 + sizeof(cf) * ((size_t)ZB * TB + N) + sizeof(uint64_t) * ZB; }
+  static_assert((XROWS * B * sizeof(cf)) % 128 == 0, "second x box off a 128-byte boundary");
 };
 
 __device__ __forceinline__ cf ldcg_cf(const cf* p) {
@@ -99,41 +113,73 @@ __device__ __forceinline__ void xy_signal(uint32_t* p) {
 
 // Op (by value) describes the batch:
 //   int grids() const                         grids per job
-//   int nsrc(int r) const                     spectra combined into each grid of radius r
-//   const cf* src(int r, int g, int i) const  spectrum i of grid g (layout S[kz][x][y])
-//   float coef(int r, int i) const            its coefficient
 //   bool filtered(int r) const                radius r is windowed
 //   const float* wrow(int r) const            its window row W[n2]
 //   int cutoff(int r) const                   >= -1: the row is the step W = (n2 <= cutoff), read
 //                                             without gathers (sharp-k); < -1: read the row
 //   cf* out(int r, int g) const               output grid (plane kz at kz N^2)
-// The X input of grid g is W(k) * sum_i coef_i src_i(k), accumulated in the order of i with fmaf.
+// The X input of grid g is W(k) * spectrum_g(k); the spectra are the tensor `smap` (floats, y
+// innermost, then x, then kz of grid g at g (N/2 + 1) + kz).
 template <int N, class Op>
 __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
-    k_xy_fused(XYSched sch, Op op, const cf* __restrict__ g_tw) {
-  constexpr int T = XYF<N>::T, B = XYF<N>::B, V = XYF<N>::V;
-  extern __shared__ cf smem[];
-  cf* s_tw = smem;
-  cf* xbuf = smem + N;
+    k_xy_fused(XYSched sch, Op op, const __grid_constant__ CUtensorMap smap, const cf* __restrict__ g_tw) {
+  using F = XYF<N>;
+  constexpr int T = F::T, B = F::B, V = F::V, TB = F::TB, NZ = N / 2 + 1;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* sm = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  cf* bufs = reinterpret_cast<cf*>(sm);
+  cf* s_tw = bufs + F::ZB * TB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
   __shared__ int s_item[2];
+  __shared__ int s_pref[2];   // the next item's first tile is in flight
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < F::ZB; ++b) mbar_init(&bars[b], 1);
+    mbar_init_fence();
+  }
   load_twiddles<N>(s_tw, g_tw);
-  if (threadIdx.x == 0) s_item[0] = (int)atomicAdd(sch.ctr, 1u);
+  if (threadIdx.x == 0) {
+    s_item[0] = (int)atomicAdd(sch.ctr, 1u);
+    s_pref[0] = 0;
+  }
   __syncthreads();
+  const int ng = op.grids();
+  // thread 0: the tile of grid g for the X item `itm` into buffer b
+  auto issue = [&](int itm, int g, int b) {
+    const int seg = itm / sch.M, k = itm - seg * sch.M;
+    bool is_y;
+    int job;
+    xy_decode(sch, seg, is_y, job);
+    const int kz = job / sch.nr;
+    mbar_arrive_expect_tx(&bars[b], F::TX);
+#pragma unroll
+    for (int xb = 0; xb < F::NXB; ++xb)
+      tma_load_3d(bufs + b * TB + xb * F::XROWS * B, &smap, 2 * k * B, xb * F::XROWS, g * NZ + kz, &bars[b]);
+  };
+  auto is_x_item = [&](int itm) {
+    if (itm >= sch.total) return false;
+    bool is_y;
+    int job;
+    xy_decode(sch, itm / sch.M, is_y, job);
+    return !is_y;
+  };
   int it = 0;
   int item = s_item[0];
-  const int ng = op.grids();
+  uint32_t xu = 0;          // X units (item, grid) this block has started: unit u uses buffer u & 1
+  bool waited = true;
   while (item < sch.total) {
     int nxt = 0;
     if (threadIdx.x == 0) nxt = (int)atomicAdd(sch.ctr, 1u);   // the next item, fetched early
+    const bool pref = s_pref[it & 1] != 0;
     const int seg = item / sch.M, k = item - seg * sch.M;
     bool is_y;
     int job;
     xy_decode(sch, seg, is_y, job);
     const int kz = job / sch.nr, r = job - kz * sch.nr;
     const size_t plane = (size_t)kz * N * N;
+    int next_pref = 0;
     if (!is_y) {
-      const int b = threadIdx.x % B, t = threadIdx.x / B;
-      const int y = k * B + b;
+      const int bcol = threadIdx.x % B, t = threadIdx.x / B;
+      const int y = k * B + bcol;
       const size_t col = plane + y;
       float wv[V];
 #pragma unroll
@@ -150,24 +196,31 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
           wv[sl] = cut >= -1 ? (n2 <= cut ? 1.f : 0.f) : __ldg(wr + n2);
         }
       }
-      const int ns = op.nsrc(r);
-      for (int g = 0; g < ng; ++g) {
+      for (int g = 0; g < ng; ++g, ++xu) {
+        const int b = (int)(xu & 1u);
+        if (threadIdx.x == 0) {
+          if (g == 0 && !pref) issue(item, 0, b);
+          // the next unit's tile into the other buffer (its previous unit has ended)
+          if (g + 1 < ng) {
+            issue(item, g + 1, b ^ 1);
+          } else if (is_x_item(nxt)) {
+            issue(nxt, 0, b ^ 1);
+            next_pref = 1;
+          }
+        }
+        if (!mbar_wait(&bars[b], (xu >> 1) & 1u, 1 << 22)) waited = false;
+        cf* tile = bufs + b * TB;
         cf* dst = op.out(r, g);
         line_fft<N, true>(
-            t, xbuf, s_tw,
+            t, tile, s_tw,
             [&](int p, int sl) {
-              float ax = 0.f, ay = 0.f;
-              for (int i = 0; i < ns; ++i) {
-                const float c = op.coef(r, i);
-                const float2 v = __ldg(reinterpret_cast<const float2*>(op.src(r, g, i) + col + (size_t)p * N));
-                ax = fmaf(c, v.x, ax);
-                ay = fmaf(c, v.y, ay);
-              }
-              return cf{ax * wv[sl], ay * wv[sl]};
+              const cf v = tile[p * B + bcol];
+              return cf{v.x * wv[sl], v.y * wv[sl]};
             },
-            [&](int p) { return line_addr<N, B>(p, b); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
+            [&](int p) { return line_addr<N, B>(p, bcol); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
+        fence_proxy_async_smem();
+        __syncthreads();   // every store of the unit is issued; its buffer may be refilled
       }
-      __syncthreads();   // every store of the item is issued
       if (threadIdx.x == 0 && sch.signal) xy_signal(sch.done + job);
     } else {
       if (threadIdx.x == 0) xy_wait(sch, job);
@@ -177,25 +230,38 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
       for (int g = 0; g < ng; ++g) {
         cf* line = op.out(r, g) + row;
         line_fft<N, true>(
-            t, xbuf, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return pos_addr<N>(b, p); },
+            t, bufs, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return pos_addr<N>(b, p); },
             [&](int p, cf v) { line[p] = v; });
       }
+      fence_proxy_async_smem();   // the exchange buffer is a tile buffer of later X items
     }
-    if (threadIdx.x == 0) s_item[(it + 1) & 1] = nxt;
+    if (threadIdx.x == 0) {
+      s_item[(it + 1) & 1] = nxt;
+      s_pref[(it + 1) & 1] = next_pref;
+    }
     __syncthreads();
     ++it;
     item = s_item[it & 1];
   }
+  if (!waited && threadIdx.x % 32 == 0) atomicExch(sch.err, 1u);
 }
 
 // Launch the fused pass of one batch of nr radii (or shells); the control words must have been
 // sized by xy_ctrl_reset for at least (N/2 + 1) nr jobs.
 template <int N, class Op>
-int launch_xy_fused(rg_context* ctx, const Op& op, int nr, const char* name, double alg_bytes, cudaStream_t st) {
+int launch_xy_fused(rg_context* ctx, const Op& op, const cf* spec, int nspec, int nr, const char* name,
+                    double alg_bytes, cudaStream_t st) {
   using F = XYF<N>;
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
+  // the nspec spectra (S[kz][x][y], one after another) as a 3-D float tensor
+  CUtensorMap smap;
+  const uint64_t dims[3] = {2ull * N, (uint64_t)N, (uint64_t)Cfg<N>::NZ * nspec};
+  const uint64_t strides[2] = {8ull * N, 8ull * N * N};
+  const uint32_t box[3] = {2u * F::B, (uint32_t)F::XROWS, 1u};
+  const int mrc = tma_map_3d(&smap, spec, dims, strides, box);
+  if (mrc != 0) return set_error(ctx, RG_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(mrc) + ")");
   const int J = Cfg<N>::NZ * nr;
   if (nr < 1 || (size_t)J + 2 > ctx->xy_ctrl_elems) return set_error(ctx, RG_EINVAL, "fused x/y pass: batch too large");
   auto kern = k_xy_fused<N, Op>;
@@ -218,7 +284,7 @@ int launch_xy_fused(rg_context* ctx, const Op& op, int nr, const char* name, dou
   s.done = ctx->xy_ctrl + 2;
   RG_CUDA_TRY(ctx, cudaMemsetAsync(s.ctr, 0, sizeof(uint32_t) * ((size_t)J + 1), st));
   prof_begin(ctx, name, st);
-  kern<<<std::min(grid, s.total), F::NTH, F::smem(), st>>>(s, op, tw);
+  kern<<<std::min(grid, s.total), F::NTH, F::smem(), st>>>(s, op, smap, tw);
   prof_end(ctx, alg_bytes, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
