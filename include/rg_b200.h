@@ -287,6 +287,15 @@ int rg_smooth_grid(rg_context* ctx, double box_size, int reion_grid_dim, const f
 int rg_deposit_ngp(rg_context* ctx, double box_size, int n_gal, const float* d_pos, int n_prop,
                    const float* d_values, const double* divisors, float* const* d_grids);
 
+/* The history bookkeeping of construct_baryon_grids (src/core/reionization.c:2105-2140 shifts
+   the slots, :2470-2500 writes the snapshot's grid into slot 0) for the grids ComputeTs reads:
+   with Flag_IncludeSpinTemp, for sfr, xray_luminosity and the AGN bands Flag_IncludeAGNXray
+   uses, slot h + 1 <- slot h for h = n_hist - 2 .. 0, then slot 0 <- the current grid (device
+   pointers of g, n_hist slots of the padded size each).  Called after the snapshot's grids are
+   deposited, it leaves the histories as the reference's deposit does.  Stream-ordered on the
+   context's stream; returns without a sync. */
+int rg_push_histories(rg_context* ctx, const rg_params* p, const rg_grids* g);
+
 /* ---- per-kernel timing: CUDA events on the launching stream around every launch ---- */
 typedef struct rg_kernel_stat {
   char name[48];

@@ -11,6 +11,8 @@
 // rounding only.
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "rg_internal.h"
 #include "rg_pass.cuh"
 
@@ -119,6 +121,44 @@ int rg_deposit_ngp(rg_context* ctx, double box_size, int n_gal, const float* d_p
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(&bad, ctx->ngp_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (bad) return set_error(ctx, RG_EINVAL, "galaxy positions below the box (pos_to_ngp asserts on them)");
+  return RG_OK;
+}
+
+int rg_push_histories(rg_context* ctx, const rg_params* p, const rg_grids* g) {
+  if (!ctx || !p || !g) return RG_EINVAL;
+  if (!p->Flag_IncludeSpinTemp) return RG_OK;   // the reference keeps histories for ComputeTs only
+  if (g->n_hist < 1) return set_error(ctx, RG_EINVAL, "n_hist must be at least 1");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const int n = ctx->N;
+  const size_t npad = (size_t)n * n * 2 * (n / 2 + 1);
+  const int agn = p->Flag_IncludeAGNXray;
+  struct Kind {
+    const float* cur;
+    float* hist;
+    bool on;
+    const char* name;
+  } kinds[4] = {  // the histories are inputs of the step (const in rg_grids); this call updates them
+      {g->sfr, const_cast<float*>(g->sfr_histories), true, "sfr"},
+      {g->xray_luminosity, const_cast<float*>(g->xray_luminosity_histories), true, "xray_luminosity"},
+      {g->bh_xray_soft, const_cast<float*>(g->bh_xray_histories_soft), agn == 1 || agn == 3, "bh_xray_soft"},
+      {g->bh_xray_hard, const_cast<float*>(g->bh_xray_histories_hard), agn == 1 || agn == 2, "bh_xray_hard"}};
+  for (const Kind& k : kinds) {
+    if (!k.on) continue;
+    if (!k.cur || !k.hist) return set_error(ctx, RG_EINVAL, std::string("missing grid or histories of ") + k.name);
+  }
+  prof_begin(ctx, "push_histories", st);
+  double bytes = 0.0;
+  for (const Kind& k : kinds) {
+    if (!k.on) continue;
+    // slot h + 1 <- slot h from the top, then slot 0 <- this snapshot's grid
+    for (int h = g->n_hist - 2; h >= 0; --h)
+      RG_CUDA_TRY(ctx, cudaMemcpyAsync(k.hist + (size_t)(h + 1) * npad, k.hist + (size_t)h * npad,
+                                       sizeof(float) * npad, cudaMemcpyDeviceToDevice, st));
+    RG_CUDA_TRY(ctx, cudaMemcpyAsync(k.hist, k.cur, sizeof(float) * npad, cudaMemcpyDeviceToDevice, st));
+    bytes += 8.0 * npad * g->n_hist;
+  }
+  prof_end(ctx, bytes, st);
   return RG_OK;
 }
 

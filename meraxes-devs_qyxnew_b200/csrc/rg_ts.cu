@@ -247,17 +247,26 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, (x_pass_minb<N>()))
     const int G = bt.ng;
     for (int g = 0; g < G; ++g) {
       cf* dst = work + ((size_t)r * G + g) * stride;
+      // the combination sum_i c_i spec_i of this thread's V input positions, source by source:
+      // the V loads of a source are independent and in flight together (per element the same
+      // fmaf sequence in the order of i)
+      cf in[V];
+#pragma unroll
+      for (int sl = 0; sl < V; ++sl) in[sl] = cf{0.f, 0.f};
+      for (int i = 0; i < nk; ++i) {
+        const float c = bt.cs[r][i];
+        const cf* src = spec + ((size_t)bt.ks[r][i] * G + g) * stride + col;
+        cf v[V];
+#pragma unroll
+        for (int sl = 0; sl < V; ++sl) v[sl] = src[(size_t)stage0_pos<N>(t, sl) * N];
+#pragma unroll
+        for (int sl = 0; sl < V; ++sl) {
+          in[sl].x = fmaf(c, v[sl].x, in[sl].x);
+          in[sl].y = fmaf(c, v[sl].y, in[sl].y);
+        }
+      }
       line_fft<N, true>(
-          t, xbuf, s_tw,
-          [&](int p, int sl) {
-            float ax = 0.f, ay = 0.f;
-            for (int i = 0; i < nk; ++i) {
-              const cf v = spec[((size_t)bt.ks[r][i] * G + g) * stride + col + (size_t)p * N];
-              ax = fmaf(bt.cs[r][i], v.x, ax);
-              ay = fmaf(bt.cs[r][i], v.y, ay);
-            }
-            return cf{ax * wv[sl], ay * wv[sl]};
-          },
+          t, xbuf, s_tw, [&](int, int sl) { return cf{in[sl].x * wv[sl], in[sl].y * wv[sl]}; },
           [&](int p) { return line_addr<N, B>(p, b); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
     }
   }

@@ -115,6 +115,7 @@ _SIGS = {
     "rg_set_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "rg_set_radius_batch": (C.c_int, [C.c_void_p, C.c_int]),
     "rg_debug_set_wait_limits": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "rg_push_histories": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_grids)]),
     "rg_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rg_last_error": (C.c_char_p, [C.c_void_p]),
     "rg_status_string": (C.c_char_p, [C.c_int]),

@@ -6,6 +6,8 @@ order, so a cell may differ by float rounding of its sum: the bound is 1e-5 of t
 absolute values that went into the cell (divided like the cell).  Every cell index is exact
 (positions that round differently would leave a whole galaxy's value in the wrong cell)."""
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -78,3 +80,36 @@ def test_deposit_rejects_positions_below_box_and_stays_usable():
     ix, iy, iz = go.pos_to_ngp(np.array([1.0, 2.0, 3.0], np.float32), box, n)
     assert h[ix, iy, iz] == 1.0 and h.sum() == 1.0
     ctx.close()
+
+
+@pytest.mark.parametrize("agn", [0, 1])
+def test_push_histories_matches_reference_shift(agn):
+    """rg_push_histories: the slot shift of construct_baryon_grids (reionization.c:2105-2140) and
+    the snapshot's grid into slot 0 (:2470-2500), for sfr, xray_luminosity and the AGN bands."""
+    import torch
+    n, nh = 16, 5
+    npad = n * n * 2 * (n // 2 + 1)
+    rng = np.random.default_rng(5 + agn)
+    names = ["sfr", "xray_luminosity"] + (["bh_xray_soft", "bh_xray_hard"] if agn else [])
+    hists = {"sfr": "sfr_histories", "xray_luminosity": "xray_luminosity_histories",
+             "bh_xray_soft": "bh_xray_histories_soft", "bh_xray_hard": "bh_xray_histories_hard"}
+    cur = {k: rng.random(npad).astype(np.float32) for k in names}
+    hist = {k: rng.random(nh * npad).astype(np.float32) for k in names}
+    dcur = {k: torch.from_numpy(v).cuda() for k, v in cur.items()}
+    dhist = {k: torch.from_numpy(v).cuda() for k, v in hist.items()}
+    g = rg.rg_grids()
+    for k in names:
+        setattr(g, k, dcur[k].data_ptr())
+        setattr(g, hists[k], dhist[k].data_ptr())
+    g.n_hist = nh
+    p = rg.make_params(n, 20.0, Flag_IncludeSpinTemp=1, Flag_IncludeAGNXray=agn)
+    ctx = rg.Context(n)
+    assert ctx.lib.rg_push_histories(ctx.h, C.byref(p), C.byref(g)) == rg.RG_OK
+    torch.cuda.synchronize()
+    ctx.close()
+    for k in names:
+        want = hist[k].reshape(nh, npad).copy()
+        for s in range(nh - 2, -1, -1):       # the reference's loop, slot s + 1 <- slot s
+            want[s + 1] = want[s]
+        want[0] = cur[k]
+        assert np.array_equal(dhist[k].cpu().numpy().reshape(nh, npad), want), k
