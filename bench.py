@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the timings reported under extras")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-extra", choices=["dft_y_pass_256"],
+                    help="run only this extra timing on one GPU and print it (for profiling)")
     return ap.parse_args()
 
 
@@ -352,7 +354,8 @@ def run_reference(args, cfg):
     desc = (cs.desc + f"; each timed step is one sample, a radius or a shell in turn ({sample_ms / 1e3:.2f} s "
             f"wall on average), the snapshot value is extrapolated from the samples and the once-per-snapshot "
             f"parts ({fixed_wall:.1f} s wall, timed before the warm-up); oracle restatement, scipy pocketfft "
-            "float32, all host cores (the reference needs FFTW/GSL/MPI, absent here)")
+            "float32, all host cores (the reference's path needs FFTW, GSL, MPI and HDF5, absent here; its "
+            "C compiled over in-tree stand-ins pins the oracle but would time a plain stand-in FFT, not FFTW)")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/snapshot", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample_ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA_DESC,
@@ -555,6 +558,41 @@ def time_recombinations(wk, ctx, torch, stream, dev):
     return res
 
 
+def time_dft_y_pass(rg, torch, dev, reps=5, ng=4):
+    """The y pass of ng whole 256^3 spectra (ng x 135 MB, above L2) by the FP32 register transform
+    and by the split-BF16 tensor-core form (rg_dft_y_pass), kernel times from the library's
+    events, and each form's relative L2 error against numpy's FP64 transform of 8 kz planes."""
+    import numpy as np
+    n, nz = 256, 129
+    ctx = rg.Context(n)
+    g = torch.Generator(device=dev).manual_seed(5)
+    base = torch.complex(torch.randn(ng * nz * n * n, device=dev, generator=g),
+                         torch.randn(ng * nz * n * n, device=dev, generator=g))
+    sample = base[: 8 * n * n].cpu().numpy().reshape(8, n, n).astype(np.complex128)
+    want = np.fft.fft(sample, axis=-1)
+    res = {}
+    for name, impl in (("fp32", rg.RG_DFT_FP32), ("tc_bf16x3", rg.RG_DFT_TC_BF16X3)):
+        work = base.clone()
+        ctx.call("rg_dft_y_pass", work.data_ptr(), 1, 0, impl)
+        got = work[: 8 * n * n].cpu().numpy().reshape(8, n, n)
+        err = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+        ctx.profile(True)
+        for _ in range(reps):
+            ctx.call("rg_dft_y_pass", work.data_ptr(), ng, 0, impl)
+        st = {k["name"]: k for k in ctx.kernel_stats()}
+        ctx.profile(False)
+        k = next(v for kname, v in st.items() if kname.startswith("dft_y"))
+        ms = k["ms_total"] / reps
+        res[name] = {"ms": ms, "GBps": k["alg_bytes_total"] / reps / (ms * 1e-3) / 1e9, "rel_l2_vs_fp64": err}
+        del work
+    ctx.close()
+    res["speedup_tc_over_fp32"] = res["fp32"]["ms"] / res["tc_bf16x3"]["ms"]
+    res["what"] = (f"one forward c2c pass along y over {ng} Hermitian 256^3 spectra (16 B per complex value "
+                   "read and written): FP32 register Stockham transform vs split-BF16 tcgen05 matrix products "
+                   "(256 = 16 x 16, three BF16 products per radix-16 stage, FP32 accumulation in tensor memory)")
+    return res
+
+
 def timed(torch, stream, fn, reset, warmup, steps):
     for _ in range(warmup):
         reset()
@@ -716,6 +754,10 @@ def run_ours(args, cfg):
     # recombination branch next to the same call without it; not part of the metric
     if not args.no_extras:
         extras["find_hii_recombinations"] = time_recombinations(wk, ctx, torch, stream, dev)
+    # the tensor-core (split-BF16 tcgen05) form of a DFT pass against the FP32 form; not part of
+    # the metric (the step uses the FP32 form)
+    if not args.no_extras:
+        extras["dft_y_pass_256"] = time_dft_y_pass(rg, torch, dev)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -759,6 +801,7 @@ def run_batch(args):
     GPU and no unit waits for another size's host round trip."""
     import threading
     import torch
+    import autotune
     import rg_b200 as rg
     import sharding
 
@@ -840,6 +883,62 @@ def run_batch(args):
             ev.record(streams[n])
             master.wait_event(ev)
 
+    # the batch entry point: one rg_find_HII_bubbles_batch call per box size and group of
+    # per_call snapshots, one host thread and stream per size; the radius batch and the group
+    # size are tuned per size (autotune.py, cached per GPU model and workload shape)
+    by_size = {n: [i for i in mine if units[i].n == n] for n in sizes}
+
+    def reset_size(n):
+        for i in by_size[n]:
+            b = state[i]["b"]
+            b["z_at_ionization"].fill_(-1.0)
+            b["J_21_at_ionization"].zero_()
+            b["temp_kinetic_all_gas"].zero_()
+
+    def run_size(n, kb, per_call):
+        ctx = ctxs[n]
+        ctx.call("rg_set_radius_batch", kb)
+        ids = by_size[n]
+        for j in range(0, len(ids), per_call):
+            grp = ids[j:j + per_call]
+            outs = ctx.find_hii_batch([state[i]["p"] for i in grp], [state[i]["s"] for i in grp],
+                                      [state[i]["g"] for i in grp])
+            for i, o in zip(grp, outs):
+                state[i]["out"] = o
+
+    gpu = torch.cuda.get_device_name(dev)
+    shape = {}
+    for n in sizes:
+        ctxs[n].call("rg_set_stream", C.c_void_p(master.cuda_stream))
+        key = autotune.shape_key(gpu, n, 2, len(by_size[n]), radii[by_size[n][0]])
+        shape[n] = autotune.tuned(key, lambda kb, pc, n=n: (reset_size(n), run_size(n, kb, pc)),
+                                  lambda: torch.cuda.synchronize(dev), len(by_size[n]))
+
+    def batch_api():
+        ev0 = torch.cuda.Event()
+        ev0.record(master)
+        for n in sizes:
+            streams[n].wait_event(ev0)
+            ctxs[n].call("rg_set_stream", C.c_void_p(streams[n].cuda_stream))
+        errs = []
+
+        def worker(n):
+            try:
+                run_size(n, *shape[n])
+            except Exception as e:      # surfaced after the join
+                errs.append(e)
+        ths = [threading.Thread(target=worker, args=(n,)) for n in sizes]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        if errs:
+            raise errs[0]
+        for n in sizes:
+            ev = torch.cuda.Event()
+            ev.record(streams[n])
+            master.wait_event(ev)
+
     def timed_ms(fn):
         for _ in range(args.warmup):
             reset()
@@ -860,16 +959,17 @@ def run_batch(args):
     if ws > 1:
         torch.distributed.barrier()
     ms_plain = sharding.max_over_ranks(timed_ms(plain))
+    ms_threads = sharding.max_over_ranks(timed_ms(batched))
     clocks = ClockSampler(local)
     clocks.start()
-    ms_batch = sharding.max_over_ranks(timed_ms(batched))
+    ms_batch = sharding.max_over_ranks(timed_ms(batch_api))
     clk = clocks.stop()
     xh = sharding.gather_scalars({i: [state[i]["out"].volume_weighted_global_xH] for i in mine}, len(units))
-    # per-kernel timing of one batched pass
+    # per-kernel timing of one pass through the batch entry point
     for c in ctxs.values():
         c.profile(True)
     reset()
-    batched()
+    batch_api()
     torch.cuda.synchronize(dev)
     stats = {}
     for c in ctxs.values():
@@ -891,8 +991,14 @@ def run_batch(args):
                                        "128^3, 192^3 (12 each, L = N Mpc/h), efficiency calibrated for <xH> 0.99 -> 0.1",
                            "name": "c2_batch", "parallelism": f"units placed whole on {ws} rank(s)",
                            "l2": "flushed (512 MiB write) before every timed step"},
+                "what": "rg_find_HII_bubbles_batch: per box size, groups of snapshots in one call (shared "
+                        "forward and x/y launches), one host thread and stream per size, launch shape tuned",
+                "tuned": {str(n): {"radius_batch": shape[n][0], "per_call": shape[n][1]} for n in sizes},
                 "plain": {"value": len(units) / (ms_plain * 1e-3), "ms_per_step": ms_plain,
-                          "what": "units one after another on one stream"},
+                          "what": "rg_find_HII_bubbles per snapshot, one after another on one stream"},
+                "per_snapshot_threads": {"value": len(units) / (ms_threads * 1e-3), "ms_per_step": ms_threads,
+                                         "what": "rg_find_HII_bubbles per snapshot, one host thread and stream "
+                                                 "per box size"},
                 "gpu_launches": sum(v[0] for v in stats.values()),
                 "roofline": {"bound": "hbm", "kernel": top[0], "achieved": ach, "peak": peak, "unit": "GB/s",
                              "frac": ach / peak, "peak_kind": peak_kind, "traffic": None},
@@ -906,6 +1012,11 @@ def run_batch(args):
 
 def main():
     args = parse()
+    if args.only_extra == "dft_y_pass_256":
+        import torch
+        import rg_b200 as rg
+        print(json.dumps({"extra": "dft_y_pass_256", **time_dft_y_pass(rg, torch, "cuda:0")}), flush=True)
+        return
     if args.config == "c2_batch":
         if args.impl == "reference":
             ws, rank, _ = dist_env()

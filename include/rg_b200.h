@@ -192,7 +192,9 @@ typedef struct rg_context rg_context;
 int rg_create(int device, int grid_dim, rg_context** out);
 int rg_destroy(rg_context* ctx);
 int rg_set_mode(rg_context* ctx, int mode);
-int rg_set_radius_batch(rg_context* ctx, int radii_per_batch);   /* 0 = autotuned */
+/* Radii per batch of the fused mode's x/y and z passes: 0 = the default, 8; larger values are
+   cut to 16 (the tuner in autotune.py picks one per workload shape). */
+int rg_set_radius_batch(rg_context* ctx, int radii_per_batch);
 /* cudaStream_t to launch on (NULL = the context's own stream). */
 int rg_set_stream(rg_context* ctx, void* stream);
 const char* rg_last_error(const rg_context* ctx);
@@ -224,6 +226,19 @@ int rg_set_recombination_tables(rg_context* ctx, const double* lnGamma, int n_z,
    (:226-230,467-508,613-644); rg_set_recombination_tables must have been called. */
 int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
                         rg_hii_scalars* out);
+
+/* find_HII_bubbles for n_units independent snapshots of one ReionGridDim on device grids, in one
+   call (arrays p[n_units], s[n_units], g[n_units], out[n_units]): the forward transforms of all
+   their grids and, for every batch of radii, the windowed inverse x/y passes of all of them run
+   as shared launches; the z passes (the barrier test) run per snapshot; the host synchronises
+   once.  Each unit gets exactly what rg_find_HII_bubbles gives it.  The units must share
+   ReionGridDim (= the context's), BoxSize, ReionFilterType, the feature flags and the radius
+   schedule (RG_EINVAL otherwise).  With recombinations, Pop III sources or RG_MODE_PLAIN the
+   units run one after another.  Device memory grows with the units: n_units x (live grids) x
+   (radius batch + 1) spectra of (N/2+1) N^2 complex values.  No counterpart in the reference,
+   which runs one snapshot per call (find_HII_bubbles.c:713-747). */
+int rg_find_HII_bubbles_batch(rg_context* ctx, int n_units, const rg_params* p, const rg_snapshot* s,
+                              const rg_grids* g, rg_hii_scalars* out);
 /* _ComputeTs (src/core/ComputeTs.c:85-1554). */
 int rg_compute_Ts(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
                   rg_ts_scalars* out);
@@ -323,6 +338,22 @@ int rg_debug_filter_roundtrip(rg_context* ctx, const rg_params* p, const float* 
    rg_compute_Ts return RG_ETIMEDOUT.  A negative (poll) or non-positive (iteration) value
    restores the default; larger values are cut to the defaults. */
 int rg_debug_set_wait_limits(rg_context* ctx, int xy_poll_limit, int xy_signal, int ts_iteration_limit);
+
+/* One c2c pass along y (the contiguous axis of the library's internal spectrum layout
+   S[kz][x][y], complex64) over n_grids whole Hermitian spectra of ReionGridDim 256, in place:
+   every line (kz, x) of (N/2+1) * N is transformed, forward (exp(-2 pi i n k / N), inverse = 0)
+   or inverse (exp(+...), no 1/N), by one of two implementations:
+     RG_DFT_FP32       the FP32 register-resident transform the step's passes use;
+     RG_DFT_TC_BF16X3  the split-BF16 tensor-core form: 256 = 16 x 16, each radix-16 stage a
+                       tcgen05 matrix product of hi/lo BF16 operands (three products) with FP32
+                       accumulation in tensor memory, about 5e-6 relative error per pass.
+   spec: device pointer, 16-byte aligned, n_grids * 129 * 256 * 256 complex64.  Both forms
+   compute what the y stage of FFTW's 3-D transforms computes (find_HII_bubbles.c:351-370,
+   ComputeTs.c:480-581); this entry point exists to compare them.  ReionGridDim other than 256
+   returns RG_EUNSUPPORTED; a tensor-core wait that runs out returns RG_ETIMEDOUT. */
+#define RG_DFT_FP32 0
+#define RG_DFT_TC_BF16X3 1
+int rg_dft_y_pass(rg_context* ctx, void* spec, int n_grids, int inverse, int impl);
 
 /* Radius schedule of find_HII_bubbles: fills up to max_r radii, returns the count in *n. */
 int rg_radius_schedule(const rg_params* p, double redshift, double* radii, int max_r, int* n);

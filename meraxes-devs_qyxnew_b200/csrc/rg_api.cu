@@ -336,6 +336,8 @@ int rg_destroy(rg_context* ctx) {
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_sums) cudaFree(ctx->d_sums);
   if (ctx->h_sums) cudaFreeHost(ctx->h_sums);
+  if (ctx->batch_sums) cudaFree(ctx->batch_sums);
+  if (ctx->h_batch_sums) cudaFreeHost(ctx->h_batch_sums);
   if (ctx->d_radii) cudaFree(ctx->d_radii);
   if (ctx->ts_stage) cudaFree(ctx->ts_stage);
   if (ctx->ts_const) cudaFree(ctx->ts_const);
@@ -608,6 +610,50 @@ int rg_find_HII_bubbles(rg_context* ctx, const rg_params* p, const rg_snapshot* 
                         rg_hii_scalars* out) {
   if (!ctx || !p || !s || !g || !out || !s->ZZ) return RG_EINVAL;
   return find_hii(ctx, p, s, g, out, nullptr);
+}
+
+int rg_find_HII_bubbles_batch(rg_context* ctx, int n_units, const rg_params* p, const rg_snapshot* s,
+                              const rg_grids* g, rg_hii_scalars* out) {
+  if (!ctx || n_units < 0 || (n_units > 0 && (!p || !s || !g || !out))) return RG_EINVAL;
+  if (n_units == 0) return RG_OK;
+  for (int u = 0; u < n_units; ++u) {
+    if (!s[u].ZZ) return set_error(ctx, RG_EINVAL, "snapshot without redshifts");
+    if (p[u].ReionGridDim != p[0].ReionGridDim || p[u].BoxSize != p[0].BoxSize ||
+        p[u].ReionFilterType != p[0].ReionFilterType || p[u].Flag_IncludeSpinTemp != p[0].Flag_IncludeSpinTemp ||
+        p[u].Flag_BHFeedback != p[0].Flag_BHFeedback ||
+        p[u].Flag_IncludeRecombinations != p[0].Flag_IncludeRecombinations ||
+        p[u].UseMiniHalos != p[0].UseMiniHalos)
+      return set_error(ctx, RG_EINVAL, "batch units differ in grid size, box, filter or feature flags");
+  }
+  // recombinations, Pop III sources and the plain mode: one snapshot at a time
+  if (n_units == 1 || ctx->mode != RG_MODE_FUSED || p[0].Flag_IncludeRecombinations || p[0].UseMiniHalos) {
+    for (int u = 0; u < n_units; ++u) {
+      const int rc = find_hii(ctx, &p[u], &s[u], &g[u], &out[u], nullptr);
+      if (rc) return rc;
+    }
+    return RG_OK;
+  }
+  for (int u = 0; u < n_units; ++u) {
+    int rc = validate_common(ctx, &p[u]);
+    if (rc) return rc;
+    const rg_grids* gu = &g[u];
+    if (s[u].snapshot < 0 || s[u].snapshot >= s[u].n_snapshots)
+      return set_error(ctx, RG_EINVAL, "snapshot out of range");
+    if (p[u].ReionRtoMFilterType < 0 || p[u].ReionRtoMFilterType > 1 || p[u].ReionFilterType < 0 ||
+        p[u].ReionFilterType > 2 || !(p[u].ReionDeltaRFactor > 1.0))
+      return set_error(ctx, RG_EINVAL, "filter or radius parameters out of range");
+    if (!gu->deltax || !gu->stars || !gu->weighted_sfr || !gu->xH || !gu->r_bubble || !gu->z_at_ionization ||
+        !gu->J_21_at_ionization || !gu->temp_kinetic_all_gas)
+      return set_error(ctx, RG_EINVAL, "missing grid pointer");
+    if (p[u].Flag_IncludeSpinTemp && (!gu->x_e_box || !gu->Tk_box))
+      return set_error(ctx, RG_EINVAL, "spin temperature needs x_e_box and Tk_box");
+    if (p[u].Flag_BHFeedback && (!gu->effective_bhm || !gu->effective_bhar))
+      return set_error(ctx, RG_EINVAL, "BH feedback needs effective_bhm and effective_bhar");
+  }
+  int rc = ensure_tables(ctx, &p[0]);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  return hii_batch(ctx, n_units, p, s, g, out);
 }
 
 static int copy_grid(rg_context* ctx, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,

@@ -700,8 +700,10 @@ struct HiiZR {
   static constexpr uint32_t TX = (uint32_t)(NBOX * KZB * 2 * Q * sizeof(cf));   // bytes the boxes deliver
   static_assert(NBOX == 1 || ((NZ - KZB) * 2 * Q * sizeof(cf)) % 128 == 0, "second box off a 128-byte boundary");
   static constexpr size_t smem() { return 128 + sizeof(cf) * ((size_t)ZB * TB + N) + sizeof(uint64_t) * ZB; }
-  // resident blocks: register room for the kept grids (up to 3 x 2V floats) without spills
-  static constexpr int MINB = NTH >= 256 ? 2 : 3;
+  // resident blocks: register room for the kept grids (up to 3 x 2V floats) without spills; the
+  // closing batch also holds ten FP64 sums (three blocks still fit at 512^3)
+  template <bool FINAL>
+  static constexpr int minb() { return FINAL ? (NTH >= 256 ? 1 : (N >= 512 ? 3 : 2)) : (NTH >= 256 ? 2 : 3); }
   // the sizes it serves: power-of-two grids of 64^3 and up (at most 16 values per thread)
   static constexpr bool USED = (N == 64 || N == 128 || N == 256 || N == 512);
   static_assert(2 * V <= 64, "two state bits per cell in 64-bit masks");
@@ -709,13 +711,17 @@ struct HiiZR {
 
 constexpr int TMA_WAIT_LIMIT = 1 << 22;   // polls of an mbarrier before a wait gives up
 
-template <int N, bool SPIN, bool BH>
-__global__ void __launch_bounds__(HiiZR<N>::NTH, HiiZR<N>::MINB)
+// FINAL: the batch ends with the snapshot's last (unfiltered) radius: the partial xH of the
+// never-ionised cells, and the closing pass (temperatures, xH, FP64 sums into partials) as in
+// k_hii_z.
+template <int N, bool SPIN, bool BH, bool FINAL>
+__global__ void __launch_bounds__(HiiZR<N>::NTH, (HiiZR<N>::template minb<FINAL>()))
     k_hii_zr(const __grid_constant__ CUtensorMap tmap, const cf* __restrict__ g_tw, HiiBatch bt, HiiConst c,
              HiiState s, uint32_t* err) {
   using Z = HiiZR<N>;
   using PL = Plan<N>;
   constexpr int Q = Z::Q, V = Z::V, ZB = Z::ZB, TB = Z::TB, NZ = Z::NZ, KZB = Z::KZB, NBOX = Z::NBOX;
+  constexpr int PADW = 2 * (N / 2 + 1);
   constexpr int NG = 2 + SPIN + BH;          // deltax, stars, [x_e], [effective_bhm]
   constexpr int GX = 2, GB = 2 + SPIN;       // grid indices of x_e and effective_bhm
   extern __shared__ unsigned char smem_raw[];
@@ -748,7 +754,7 @@ __global__ void __launch_bounds__(HiiZR<N>::NTH, HiiZR<N>::MINB)
     for (int u = 0; u < ZB && u < nunits; ++u) issue(u);
 
   // state of this thread's 2V cells: cell 2 slot + h is row y0 + 2q + h at z = last_pos(tq, slot)
-  uint64_t A = 0, I = 0;
+  uint64_t A = 0, I = 0, P = 0;   // P: partly ionised at the closing radius
 #pragma unroll
   for (int slot = 0; slot < V; ++slot) {
     const int z = last_pos<PL>(tq, slot);
@@ -766,12 +772,17 @@ __global__ void __launch_bounds__(HiiZR<N>::NTH, HiiZR<N>::MINB)
     }
   }
 
+  const uint64_t A0 = A;
   float vals[NG - 1][2 * V];   // the transformed grids before the last one, for the radius in work
+  double acc[FINAL ? HII_NSUM : 1];
+#pragma unroll
+  for (int k = 0; k < (FINAL ? HII_NSUM : 1); ++k) acc[k] = 0.0;
   bool waited = true;
   int u = 0;
   for (int r = 0; r < bt.nr; ++r) {
     const double pref = bt.fcoll_pref[r];
     const float jaux = bt.J_aux[r], jaux_bh = bt.J_aux_bh[r];
+    const bool lastr = FINAL && r == bt.nr - 1;
     // one (radius, grid) unit; the grid index is a compile-time constant (register arrays)
     auto unit = [&](auto gconst) {
       constexpr int g = decltype(gconst)::value;
@@ -814,19 +825,34 @@ __global__ void __launch_bounds__(HiiZR<N>::NTH, HiiZR<N>::MINB)
                 const double num = BH ? (double)bhm + (double)st : (double)st;
                 const bool ion = num * pref > nf * (1.0 + 0.0) * dom;
                 const uint64_t bit = 1ull << (2 * slot + h);
+                const size_t cellrow = (size_t)x * N + y0 + 2 * q + h;
+                const size_t ir = cellrow * N + z;
+                float xH = (I & bit) ? 0.f : 1.f;   // so far: 0 once ionized at a radius, else 1
                 if (ion) {
                   I |= bit;
-                  if (A & bit) {
-                    // new ionization (find_HII_bubbles.c:531-543)
-                    A &= ~bit;
-                    const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
-                    s.z_in[ir] = c.redshift;
-                    if (c.uvb == 1) {
-                      float j = st * jaux;
-                      if (BH) j += bhm * jaux_bh;
-                      s.J21[ir] = j;
-                    }
+                  xH = 0.f;
+                } else if (lastr && xH > REL_TOL) {
+                  // partially ionized: xH = nf - f_coll prefactor; its temperature is that of the
+                  // neutral gas (the closing pass below)
+                  P |= bit;
+                  const double fcs = (double)st / dom;
+                  const double fbh = BH ? (double)bhm / dom : 0.0;
+                  const float v = (float)(nf - (fbh + fcs) * pref);
+                  xH = v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+                }
+                if (xH < REL_TOL && (A & bit)) {
+                  // new ionization (find_HII_bubbles.c:531-543)
+                  A &= ~bit;
+                  s.z_in[ir] = c.redshift;
+                  if (c.uvb == 1) {
+                    float j = st * jaux;
+                    if (BH) j += bhm * jaux_bh;
+                    s.J21[ir] = j;
                   }
+                }
+                // the cell's deltax is used: its register keeps the final xH for the closing pass
+                if constexpr (FINAL) {
+                  if (lastr) vals[0][2 * slot + h] = xH;
                 }
               }
             }
@@ -841,23 +867,78 @@ __global__ void __launch_bounds__(HiiZR<N>::NTH, HiiZR<N>::MINB)
     for_each_index(std::make_integer_sequence<int, NG>{}, unit);
   }
   if (!waited && threadIdx.x % 32 == 0) atomicExch(err, 1u);
+  if constexpr (FINAL) {
+    // closing pass (find_HII_bubbles.c:577-645) of this thread's cells, four slots at a time with
+    // their loads issued together.  z_at_ionization is this snapshot's redshift where this batch
+    // set it (A0 & ~A), else it is read (not written by this kernel).  A partly ionised cell's
+    // temperature, ComputePartiallyIoinizedTemperature of the neutral gas's T at residual xH 1,
+    // is that T: Tk_box with the spin temperature, else the adiabatic T; the floor is the same T.
+    constexpr int CH = 4;
 #pragma unroll
-  for (int slot = 0; slot < V; ++slot) {
-    const int z = last_pos<PL>(tq, slot);
+    for (int s0 = 0; s0 < V; s0 += CH) {
+      float du[2 * CH], tk[2 * CH], tp[2 * CH], zi[2 * CH], ws[2 * CH], bh[2 * CH];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
-      const int sh = 2 * slot + h;
-      s.st8[ir] = (uint8_t)(((A >> sh) & 1ull) | (((I >> sh) & 1ull) << 1));
+      for (int j = 0; j < 2 * CH; ++j) {
+        const int slot = s0 + j / 2, h = j % 2;
+        const uint64_t bit = 1ull << (2 * slot + h);
+        const size_t cellrow = (size_t)x * N + y0 + 2 * q + h;
+        const int z = last_pos<PL>(tq, slot);
+        const size_t ir = cellrow * N + z, ip = cellrow * PADW + z;
+        const float xH = vals[0][2 * slot + h];
+        du[j] = s.deltax_unf[ip];
+        ws[j] = s.wsfr[ip];
+        bh[j] = s.bhar != nullptr ? s.bhar[ip] : 0.f;
+        tk[j] = SPIN ? s.Tk_box[ir] : 0.f;
+        tp[j] = (P & bit) ? 0.f : s.temp[ir];
+        zi[j] = (xH < REL_TOL && !((A0 & ~A) & bit)) ? s.z_in[ir] : c.redshift;
+      }
+#pragma unroll
+      for (int j = 0; j < 2 * CH; ++j) {
+        const int slot = s0 + j / 2, h = j % 2;
+        const uint64_t bit = 1ull << (2 * slot + h);
+        const size_t cellrow = (size_t)x * N + y0 + 2 * q + h;
+        const size_t ir = cellrow * N + last_pos<PL>(tq, slot);
+        const float xH = vals[0][2 * slot + h];
+        const float tn = SPIN ? tk[j] : (float)((double)c.TK * (1.0 + (double)(c.cT_ad * du[j])));
+        float temp = (P & bit) ? tn : tp[j];
+        if (xH < REL_TOL && zi[j] > 0.f) temp = fully_ionized_T(zi[j], c.redshift, du[j]);
+        if (temp < tn) temp = tn;
+        s.xH[ir] = xH;
+        s.temp[ir] = temp;
+        const double domu = 1.0 + (double)du[j];
+        acc[0] += (double)xH;
+        acc[2] += (double)ws[j];
+        acc[3] += (double)bh[j];
+        acc[4] += (double)temp;
+        acc[5] += (double)xH * domu;
+        acc[7] += (double)temp * domu;
+        acc[8] += domu;
+      }
+    }
+    block_sum<Z::NTH, HII_NSUM>(acc, s.partials + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * HII_NSUM);
+  } else {
+#pragma unroll
+    for (int slot = 0; slot < V; ++slot) {
+      const int z = last_pos<PL>(tq, slot);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const size_t ir = ((size_t)x * N + y0 + 2 * q + h) * N + z;
+        const int sh = 2 * slot + h;
+        s.st8[ir] = (uint8_t)(((A >> sh) & 1ull) | (((I >> sh) & 1ull) << 1));
+      }
     }
   }
 }
 
 // the batch of the fused x/y pass: grid g of spec windowed for radius r into work (r ng + g)
+// The grids may be several snapshots' (ngu grids each, the same radii): the work buffer holds
+// snapshot u's block [radius][its grids] at u nr ngu (one snapshot: [radius][grid]).
 struct HiiXOp {
   const cf* spec;
   size_t stride;
   int ng;
+  int ngu;           // grids per snapshot
+  int nr;            // radii of the batch
   cf* work;
   const float* wrows;
   int wpitch;
@@ -867,21 +948,25 @@ struct HiiXOp {
   __device__ bool filtered(int r) const { return r != unfiltered; }
   __device__ const float* wrow(int r) const { return wrows + (size_t)r * wpitch; }
   __device__ int cutoff(int r) const { return wcut ? __ldg(wcut + r) : -2; }
-  __device__ cf* out(int r, int g) const { return work + ((size_t)r * ng + g) * stride; }
+  __device__ cf* out(int r, int g) const {
+    const int u = g / ngu;
+    return work + (((size_t)u * nr + r) * ngu + (g - u * ngu)) * stride;
+  }
 };
 
 // inverse x (window, batch of nr radii) and y passes: one fused kernel, or (plain mode) the two
 // passes as separate kernels
 template <int N>
-int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, cf* work, size_t stride, int nr, const float* wrows,
-                      int wpitch, int unfiltered, cudaStream_t st, const int* wcut = nullptr) {
+int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, int ngu, cf* work, size_t stride, int nr,
+                      const float* wrows, int wpitch, int unfiltered, cudaStream_t st, const int* wcut = nullptr) {
   using C = Cfg<N>;
   const double nzc = (double)C::NZ * N * N;
   if (ctx->mode == RG_MODE_FUSED) {
-    const HiiXOp op{spec, stride, ng, work, wrows, wpitch, unfiltered, wcut};
+    const HiiXOp op{spec, stride, ng, ngu, nr, work, wrows, wpitch, unfiltered, wcut};
     if (stride != (size_t)C::NZ * N * N) return set_error(ctx, RG_EINVAL, "fused x/y pass: spectra must be contiguous");
     return launch_xy_fused<N>(ctx, op, spec, ng, nr, "inv_xy_c2c_window", ng * 8.0 * nzc * (1 + nr), st);
   }
+  if (ngu != ng) return set_error(ctx, RG_EINVAL, "several snapshots in one pass need the fused mode");
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
@@ -934,7 +1019,7 @@ int launch_hii_z3(rg_context* ctx, const cf* work, size_t stride, const HiiBatch
   return RG_OK;
 }
 
-template <int N, bool SPIN, bool BH>
+template <int N, bool SPIN, bool BH, bool FINAL>
 int launch_hii_zr3(rg_context* ctx, const cf* work, const HiiBatch& bt, const HiiConst& c, const HiiState& s,
                    cudaStream_t st, int* nblocks) {
   using Z = HiiZR<N>;
@@ -949,14 +1034,17 @@ int launch_hii_zr3(rg_context* ctx, const cf* work, const HiiBatch& bt, const Hi
   const uint32_t box[3] = {4u * Z::Q, 1u, (uint32_t)Z::KZB};
   const int mrc = tma_map_3d(&map, work, dims, strides, box);
   if (mrc != 0) return set_error(ctx, RG_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(mrc) + ")");
-  auto kern = k_hii_zr<N, SPIN, BH>;
+  auto kern = k_hii_zr<N, SPIN, BH, FINAL>;
   RG_CUDA_TRY(ctx, prep(kern, Z::smem()));
   const dim3 grid(N / (2 * Z::Q), N);
   const double n3 = (double)N * N * N, nzc = (double)Z::NZ * N * N;
   // algorithmic bytes: the Hermitian halves of NG grids per radius, the state (z_at_ionization on
-  // the first batch, one byte per cell read otherwise, one written)
-  const double bytes = bt.nr * NG * 8.0 * nzc + (bt.first ? 4.0 * n3 : 1.0 * n3) + 1.0 * n3;
-  prof_begin(ctx, "inv_z_c2r_test", st);
+  // the first batch, one byte per cell read otherwise, one written before the closing batch); the
+  // closing pass writes xH and temperature and reads deltax, weighted_sfr, [effective_bhar], the
+  // temperature and [Tk_box]
+  double bytes = bt.nr * NG * 8.0 * nzc + (bt.first ? 4.0 * n3 : 1.0 * n3) + (FINAL ? 0.0 : 1.0 * n3);
+  if (FINAL) bytes += 4.0 * n3 * (2 + 3 + (s.bhar != nullptr) + SPIN);
+  prof_begin(ctx, FINAL ? "inv_z_c2r_test_final" : "inv_z_c2r_test", st);
   kern<<<grid, Z::NTH, Z::smem(), st>>>(map, tw, bt, c, s, ctx->xy_ctrl);
   prof_end(ctx, bytes, st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
@@ -967,13 +1055,19 @@ int launch_hii_zr3(rg_context* ctx, const cf* work, const HiiBatch& bt, const Hi
 template <int N>
 int launch_hii_z(rg_context* ctx, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
                  const HiiState& s, bool fin, cudaStream_t st, int* nblocks) {
-  // batches before the last one without recombinations or Pop III: TMA tiles, registers
+  // without recombinations or Pop III: TMA tiles, registers
   if constexpr (HiiZR<N>::USED) {
-    if (!fin && !c.rec && !c.mini) {
-      if (c.spin && c.bh) return launch_hii_zr3<N, true, true>(ctx, work, bt, c, s, st, nblocks);
-      if (c.spin) return launch_hii_zr3<N, true, false>(ctx, work, bt, c, s, st, nblocks);
-      if (c.bh) return launch_hii_zr3<N, false, true>(ctx, work, bt, c, s, st, nblocks);
-      return launch_hii_zr3<N, false, false>(ctx, work, bt, c, s, st, nblocks);
+    if (!c.rec && !c.mini) {
+      if (fin) {
+        if (c.spin && c.bh) return launch_hii_zr3<N, true, true, true>(ctx, work, bt, c, s, st, nblocks);
+        if (c.spin) return launch_hii_zr3<N, true, false, true>(ctx, work, bt, c, s, st, nblocks);
+        if (c.bh) return launch_hii_zr3<N, false, true, true>(ctx, work, bt, c, s, st, nblocks);
+        return launch_hii_zr3<N, false, false, true>(ctx, work, bt, c, s, st, nblocks);
+      }
+      if (c.spin && c.bh) return launch_hii_zr3<N, true, true, false>(ctx, work, bt, c, s, st, nblocks);
+      if (c.spin) return launch_hii_zr3<N, true, false, false>(ctx, work, bt, c, s, st, nblocks);
+      if (c.bh) return launch_hii_zr3<N, false, true, false>(ctx, work, bt, c, s, st, nblocks);
+      return launch_hii_zr3<N, false, false, false>(ctx, work, bt, c, s, st, nblocks);
     }
   }
   // with recombinations or Pop III (up to 9 grids) one instantiation reads the count from the
@@ -1003,7 +1097,7 @@ int launch_debug_inverse(rg_context* ctx, const cf* spec, cf* work, const float*
   const size_t stride = (size_t)Cfg<N>::NZ * N * N;
   int rc = xy_ctrl_reset(ctx, Cfg<N>::NZ, st);
   if (rc) return rc;
-  rc = launch_inverse_xy<N>(ctx, spec, 1, work, stride, 1, wrow, 0, wrow ? -1 : 0, st);
+  rc = launch_inverse_xy<N>(ctx, spec, 1, 1, work, stride, 1, wrow, 0, wrow ? -1 : 0, st);
   if (rc) return rc;
   const cf* tw;
   if ((rc = twiddles_for(ctx, N, &tw))) return rc;
@@ -1055,9 +1149,9 @@ int fft_forward(rg_context* ctx, int n, const float* const* d_real, int ng, cf* 
   RG_DISPATCH_N(n, launch_forward<NN>(ctx, d_real, ng, spec, stride, scale, st));
 }
 
-static int inverse_xy(rg_context* ctx, int n, const cf* spec, int ng, cf* work, size_t stride, int nr,
+static int inverse_xy(rg_context* ctx, int n, const cf* spec, int ng, int ngu, cf* work, size_t stride, int nr,
                       const float* wrows, int wpitch, int unfiltered, cudaStream_t st, const int* wcut) {
-  RG_DISPATCH_N(n, launch_inverse_xy<NN>(ctx, spec, ng, work, stride, nr, wrows, wpitch, unfiltered, st, wcut));
+  RG_DISPATCH_N(n, launch_inverse_xy<NN>(ctx, spec, ng, ngu, work, stride, nr, wrows, wpitch, unfiltered, st, wcut));
 }
 
 static int hii_z(rg_context* ctx, int n, const cf* work, size_t stride, int ng, const HiiBatch& bt, const HiiConst& c,
@@ -1110,38 +1204,62 @@ int xy_ctrl_check(rg_context* ctx, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // the snapshot
 
-int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out,
-                 const Staging* stg) {
-  const Staging none;
-  if (!stg) stg = &none;
-  int rc;
-  cudaStream_t st = ctx->stream;
-  const int N = ctx->N;
-  const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
-  const bool rec = p->Flag_IncludeRecombinations != 0;
-  const bool mini = p->UseMiniHalos != 0;
-  const double redshift = s->ZZ[s->snapshot];
-  const double box_size = p->BoxSize;
-  const double pixel_volume = std::pow(box_size / (double)N, 3);
-  const Units u = make_units(p);
-  const double sfr_timescale = p->ReionSfrTimescale * hubble_time_at(p, redshift);
+// per-snapshot constants of the z passes
+static int hii_const(rg_context* ctx, const rg_params* p, double redshift, HiiConst* c) {
   const double tk_d = T_RECFAST(ctx->tables, (float)redshift);
   if (tk_d < 0) return set_error(ctx, RG_ETABLE, "T_RECFAST called beyond its table");
-  HiiConst c;
-  c.redshift = (float)redshift;
-  c.TK = (float)tk_d;
-  c.cT_ad = cT_approx((float)redshift);
-  c.uvb = p->ReionUVBFlag;
-  c.spin = spin;
-  c.bh = bh;
-  c.rec = rec;
-  c.mini = mini;
+  c->redshift = (float)redshift;
+  c->TK = (float)tk_d;
+  c->cT_ad = cT_approx((float)redshift);
+  c->uvb = p->ReionUVBFlag;
+  c->spin = p->Flag_IncludeSpinTemp != 0;
+  c->bh = p->Flag_BHFeedback != 0;
+  c->rec = p->Flag_IncludeRecombinations != 0;
+  c->mini = p->UseMiniHalos != 0;
+  return RG_OK;
+}
 
-  // Grids to transform: the ones the z pass reads, in its order.  weighted_sfr (and
-  // effective_bhar) feed only Gamma12 on the recombination branch, so without it their
-  // filtered fields are never read; the plain mode transforms weighted_sfr anyway, as the
-  // reference does.
-  const float* srcs[10];
+// the per-radius prefactors of radii [r0, r0 + cnt) (find_HII_bubbles.c:430-450)
+static void hii_batch_radii(const rg_params* p, double redshift, const std::vector<std::pair<double, bool>>& sched,
+                            int r0, int cnt, int ntest, HiiBatch* bt) {
+  const int N = p->ReionGridDim;
+  const double pixel_volume = std::pow(p->BoxSize / (double)N, 3);
+  const Units u = make_units(p);
+  const double sfr_timescale = p->ReionSfrTimescale * hubble_time_at(p, redshift);
+  std::memset(bt, 0, sizeof(*bt));
+  bt->nr = cnt;
+  bt->first = (r0 == 0);
+  bt->ng = ntest;
+  for (int k = 0; k < cnt; ++k) {
+    const double R = sched[r0 + k].first;
+    const double M_mean = rtom(p, R);
+    double Gamma_R_prefactor = (1.0 + redshift) * (1.0 + redshift) * R * p->UnitLength_in_cm / pixel_volume *
+                               std::pow(p->UnitLength_in_cm, -3.);
+    Gamma_R_prefactor *= (p->UnitMass_in_g / u.UnitTime_in_s) / PROTONMASS * p->ReionNionPhotPerBary;
+    bt->J_aux[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
+                           p->ReionAlphaUV);
+    bt->J_aux_bh[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias /
+                              sfr_timescale * p->ReionAlphaUVBH);
+    const double G_bh = Gamma_R_prefactor * (SIGMA_HI * p->ReionAlphaUVBH / (p->ReionAlphaUVBH + 2.75) * 1e12);
+    Gamma_R_prefactor *= SIGMA_HI * p->ReionAlphaUV / (p->ReionAlphaUV + 2.75) * 1e12;
+    bt->G_pref[k] = (float)Gamma_R_prefactor;
+    bt->G_pref_bh[k] = (float)G_bh;
+    bt->R[k] = (float)R;
+    bt->fcoll_pref[k] = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R * R * R;
+    // Pop III (find_HII_bubbles.c:443-450): photons per baryon and efficiency of their own
+    bt->J_auxIII[k] = bt->J_aux[k] * (float)(p->ReionNionPhotPerBaryIII / p->ReionNionPhotPerBary);
+    bt->G_prefIII[k] = (float)(Gamma_R_prefactor * p->ReionNionPhotPerBaryIII / p->ReionNionPhotPerBary);
+    bt->fcoll_prefIII[k] = bt->fcoll_pref[k] / p->ReionEfficiency * p->ReionEfficiencyIII;
+  }
+}
+
+// the grids the z pass tests, in its order (the first ntest of srcs), then in the plain mode
+// without recombinations weighted_sfr; returns the count.  weighted_sfr (and effective_bhar) feed
+// only Gamma12 on the recombination branch, so without it their filtered fields are never read;
+// the plain mode transforms weighted_sfr anyway, as the reference does.
+static int hii_sources(const rg_params* p, const rg_grids* g, bool plain, const float** srcs, int* ntest) {
+  const bool spin = p->Flag_IncludeSpinTemp != 0, bh = p->Flag_BHFeedback != 0;
+  const bool rec = p->Flag_IncludeRecombinations != 0, mini = p->UseMiniHalos != 0;
   int ng = 0;
   srcs[ng++] = g->deltax;
   srcs[ng++] = g->stars;
@@ -1154,9 +1272,93 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     if (bh) srcs[ng++] = g->effective_bhar;
     if (mini) srcs[ng++] = g->weighted_sfrIII;
   }
-  const int ntest = ng;
-  const bool plain = ctx->mode == RG_MODE_PLAIN;
+  *ntest = ng;
   if (plain && !rec) srcs[ng++] = g->weighted_sfr;
+  return ng;
+}
+
+static HiiState hii_state(const rg_params* p, const rg_grids* g, uint8_t* st8, double* partials) {
+  const bool bh = p->Flag_BHFeedback != 0, mini = p->UseMiniHalos != 0;
+  HiiState hs;
+  hs.xH = g->xH;
+  hs.z_in = g->z_at_ionization;
+  hs.J21 = g->J_21_at_ionization;
+  hs.temp = g->temp_kinetic_all_gas;
+  hs.Tk_box = p->Flag_IncludeSpinTemp ? g->Tk_box : nullptr;
+  hs.deltax_unf = g->deltax;
+  hs.wsfr = g->weighted_sfr;
+  hs.bhar = bh ? g->effective_bhar : nullptr;
+  hs.wsfrIII = mini ? g->weighted_sfrIII : nullptr;
+  hs.Gamma12 = g->Gamma12;
+  hs.r_bubble = g->r_bubble;
+  hs.st8 = st8;
+  hs.partials = partials;
+  return hs;
+}
+
+// the box averages from the reduced sums S (find_HII_bubbles.c:650-700)
+static void hii_outputs(const rg_params* p, int nr, const double* S, rg_hii_scalars* out) {
+  const bool rec = p->Flag_IncludeRecombinations != 0, mini = p->UseMiniHalos != 0;
+  const Units u = make_units(p);
+  const double n3 = std::pow((double)p->ReionGridDim, 3);
+  const double mass_weight = S[8];
+  const double to_msun_yr = p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
+  out->volume_weighted_global_xH = S[0] / n3;
+  out->volume_weighted_global_r_bubble = S[1] / n3;
+  out->volume_weighted_global_weighted_sfr = S[2] / n3 * to_msun_yr;
+  out->volume_weighted_global_effective_bhar = S[3] / n3 * to_msun_yr;
+  out->volume_weighted_global_temp_kinetic_all_gas = S[4] / n3;
+  out->mass_weighted_global_xH = S[5] / mass_weight;
+  out->mass_weighted_global_r_bubble = S[6] / mass_weight;
+  out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
+  out->n_radii = nr;
+  out->volume_weighted_global_weighted_sfrIII = mini ? S[9] / n3 * to_msun_yr : 0.0;
+  const double* R = S + 16;   // recombination sums (find_HII_bubbles.c:666-684)
+  out->volume_weighted_global_Gamma12 = rec ? R[2] / n3 : 0.0;
+  out->volume_weighted_global_N_rec = rec ? R[4] / n3 : 0.0;
+  out->volume_weighted_global_residual_xH = rec ? R[6] / n3 : 0.0;
+  out->volume_weighted_global_clumping_factor = rec ? R[8] / n3 : 0.0;
+  out->mass_weighted_global_Gamma12 = rec ? R[3] / mass_weight : 0.0;
+  out->mass_weighted_global_N_rec = rec ? R[5] / mass_weight : 0.0;
+  out->mass_weighted_global_residual_xH = rec ? R[7] / mass_weight : 0.0;
+  out->mass_weighted_global_clumping_factor = rec ? R[9] / mass_weight : 0.0;
+  if (rec) {
+    out->volume_weighted_global_r_bubble = R[0] / n3;
+    out->mass_weighted_global_r_bubble = R[1] / mass_weight;
+  }
+}
+
+// the window table of every radius (and the sharp-k steps) into ctx->wtab / ctx->wcut
+static int hii_windows(rg_context* ctx, const rg_params* p, const std::vector<std::pair<double, bool>>& sched,
+                       cudaStream_t st) {
+  const int N = ctx->N, nr = (int)sched.size();
+  const int n2max = 3 * (N / 2) * (N / 2);
+  std::vector<double> radii(nr);
+  for (int i = 0; i < nr; ++i) radii[i] = sched[i].first;
+  int rc;
+  if ((rc = ensure_device(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
+  if ((rc = ensure_device(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nr))) return rc;
+  return window_table(ctx, p->BoxSize, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st, ctx->wcut);
+}
+
+int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out,
+                 const Staging* stg) {
+  const Staging none;
+  if (!stg) stg = &none;
+  int rc;
+  cudaStream_t st = ctx->stream;
+  const int N = ctx->N;
+  const bool rec = p->Flag_IncludeRecombinations != 0;
+  const double redshift = s->ZZ[s->snapshot];
+  HiiConst c;
+  if ((rc = hii_const(ctx, p, redshift, &c))) return rc;
+
+  const float* srcs[10];
+  int ntest = 0;
+  const bool plain = ctx->mode == RG_MODE_PLAIN;
+  const int ng = hii_sources(p, g, plain, srcs, &ntest);
 
   const size_t nc = (size_t)(N / 2 + 1) * N * N;
   auto sched = radius_schedule(p, redshift);
@@ -1174,16 +1376,8 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
                           1.0 / std::pow((double)N, 3), st)))
       return rc;
 
-  // window table for all radii
+  if ((rc = hii_windows(ctx, p, sched, st))) return rc;
   const int n2max = 3 * (N / 2) * (N / 2);
-  std::vector<double> radii(nr);
-  for (int i = 0; i < nr; ++i) radii[i] = sched[i].first;
-  if ((rc = ensure_device(ctx, &ctx->d_radii, &ctx->d_radii_elems, (size_t)nr))) return rc;
-  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_radii, radii.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, st));
-  if ((rc = ensure_device(ctx, &ctx->wtab, &ctx->wtab_elems, (size_t)nr * (n2max + 1)))) return rc;
-  if ((rc = ensure_device(ctx, &ctx->wcut, &ctx->wcut_elems, (size_t)nr))) return rc;
-  if ((rc = window_table(ctx, box_size, ctx->d_radii, nr, p->ReionFilterType, ctx->wtab, n2max, st, ctx->wcut)))
-    return rc;
   const int* wcut = p->ReionFilterType == 1 ? ctx->wcut : nullptr;
 
   // r_bubble is only written on the recombination branch: zero it once
@@ -1199,21 +1393,7 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   double* partials =
       ensure_partials(ctx, std::max((size_t)N * N * HII_NSUM, (size_t)4 * ctx->num_sms * REC_NSUM));
   if (!partials) return set_error(ctx, RG_ENOMEM, "partials");
-
-  HiiState hs;
-  hs.xH = g->xH;
-  hs.z_in = g->z_at_ionization;
-  hs.J21 = g->J_21_at_ionization;
-  hs.temp = g->temp_kinetic_all_gas;
-  hs.Tk_box = spin ? g->Tk_box : nullptr;
-  hs.deltax_unf = g->deltax;
-  hs.wsfr = g->weighted_sfr;
-  hs.bhar = bh ? g->effective_bhar : nullptr;
-  hs.wsfrIII = mini ? g->weighted_sfrIII : nullptr;
-  hs.Gamma12 = g->Gamma12;
-  hs.r_bubble = g->r_bubble;
-  hs.st8 = reinterpret_cast<uint8_t*>(ctx->bits);
-  hs.partials = partials;
+  const HiiState hs = hii_state(p, g, reinterpret_cast<uint8_t*>(ctx->bits), partials);
 
   if ((rc = xy_ctrl_reset(ctx, (size_t)(N / 2 + 1) * kb, st))) return rc;
   int nblocks = 0;
@@ -1221,36 +1401,11 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
     const int cnt = std::min(kb, nr - r0);
     const bool fin = (r0 + cnt == nr);
     HiiBatch bt;
-    std::memset(&bt, 0, sizeof(bt));
-    bt.nr = cnt;
-    bt.first = (r0 == 0);
-    bt.ng = ntest;
-    for (int k = 0; k < cnt; ++k) {
-      const double R = sched[r0 + k].first;
-      const double M_mean = rtom(p, R);
-      // find_HII_bubbles.c:430-442
-      double Gamma_R_prefactor = (1.0 + redshift) * (1.0 + redshift) * R * p->UnitLength_in_cm / pixel_volume *
-                                 std::pow(p->UnitLength_in_cm, -3.);
-      Gamma_R_prefactor *= (p->UnitMass_in_g / u.UnitTime_in_s) / PROTONMASS * p->ReionNionPhotPerBary;
-      bt.J_aux[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias / sfr_timescale *
-                            p->ReionAlphaUV);
-      bt.J_aux_bh[k] = (float)(Gamma_R_prefactor * PLANCK * 1e21 / (4.0 * M_PI) * p->ReionGammaHaloBias /
-                               sfr_timescale * p->ReionAlphaUVBH);
-      const double G_bh = Gamma_R_prefactor * (SIGMA_HI * p->ReionAlphaUVBH / (p->ReionAlphaUVBH + 2.75) * 1e12);
-      Gamma_R_prefactor *= SIGMA_HI * p->ReionAlphaUV / (p->ReionAlphaUV + 2.75) * 1e12;
-      bt.G_pref[k] = (float)Gamma_R_prefactor;
-      bt.G_pref_bh[k] = (float)G_bh;
-      bt.R[k] = (float)R;
-      bt.fcoll_pref[k] = p->ReionEfficiency * (4.0 / 3.0) * M_PI / pixel_volume / M_mean * R * R * R;
-      // Pop III (find_HII_bubbles.c:443-450): photons per baryon and efficiency of their own
-      bt.J_auxIII[k] = bt.J_aux[k] * (float)(p->ReionNionPhotPerBaryIII / p->ReionNionPhotPerBary);
-      bt.G_prefIII[k] = (float)(Gamma_R_prefactor * p->ReionNionPhotPerBaryIII / p->ReionNionPhotPerBary);
-      bt.fcoll_prefIII[k] = bt.fcoll_pref[k] / p->ReionEfficiency * p->ReionEfficiencyIII;
-    }
+    hii_batch_radii(p, redshift, sched, r0, cnt, ntest, &bt);
     // the snapshot's last radius is unfiltered (find_HII_bubbles.c:313)
     const int unf = fin ? cnt - 1 : -1;
-    if ((rc = inverse_xy(ctx, N, ctx->spec, ng, ctx->work, nc, cnt, ctx->wtab + (size_t)r0 * (n2max + 1), n2max + 1,
-                         unf, st, wcut ? wcut + r0 : nullptr)))
+    if ((rc = inverse_xy(ctx, N, ctx->spec, ng, ng, ctx->work, nc, cnt, ctx->wtab + (size_t)r0 * (n2max + 1),
+                         n2max + 1, unf, st, wcut ? wcut + r0 : nullptr)))
       return rc;
     if (r0 == 0 && (rc = stage_wait(ctx, stg->state, st))) return rc;
     if (fin && (rc = stage_wait(ctx, stg->closing, st))) return rc;
@@ -1293,35 +1448,94 @@ int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, cons
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   prof_resolve(ctx);
   if ((rc = xy_ctrl_check(ctx, st))) return rc;
+  hii_outputs(p, nr, ctx->h_sums, out);
+  return RG_OK;
+}
 
-  const double n3 = std::pow((double)N, 3);
-  const double* S = ctx->h_sums;
-  const double mass_weight = S[8];
-  out->volume_weighted_global_xH = S[0] / n3;
-  out->volume_weighted_global_r_bubble = S[1] / n3;
-  out->volume_weighted_global_weighted_sfr = S[2] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
-  out->volume_weighted_global_effective_bhar =
-      S[3] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS;
-  out->volume_weighted_global_temp_kinetic_all_gas = S[4] / n3;
-  out->mass_weighted_global_xH = S[5] / mass_weight;
-  out->mass_weighted_global_r_bubble = S[6] / mass_weight;
-  out->mass_weighted_global_temp_kinetic_all_gas = S[7] / mass_weight;
-  out->n_radii = nr;
-  out->volume_weighted_global_weighted_sfrIII =
-      mini ? S[9] / n3 * p->UnitMass_in_g / u.UnitTime_in_s * SEC_PER_YEAR / SOLAR_MASS : 0.0;
-  const double* R = S + 16;   // recombination sums (find_HII_bubbles.c:666-684)
-  out->volume_weighted_global_Gamma12 = rec ? R[2] / n3 : 0.0;
-  out->volume_weighted_global_N_rec = rec ? R[4] / n3 : 0.0;
-  out->volume_weighted_global_residual_xH = rec ? R[6] / n3 : 0.0;
-  out->volume_weighted_global_clumping_factor = rec ? R[8] / n3 : 0.0;
-  out->mass_weighted_global_Gamma12 = rec ? R[3] / mass_weight : 0.0;
-  out->mass_weighted_global_N_rec = rec ? R[5] / mass_weight : 0.0;
-  out->mass_weighted_global_residual_xH = rec ? R[7] / mass_weight : 0.0;
-  out->mass_weighted_global_clumping_factor = rec ? R[9] / mass_weight : 0.0;
-  if (rec) {
-    out->volume_weighted_global_r_bubble = R[0] / n3;
-    out->mass_weighted_global_r_bubble = R[1] / mass_weight;
+int hii_batch(rg_context* ctx, int nu, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+              rg_hii_scalars* out) {
+  int rc;
+  cudaStream_t st = ctx->stream;
+  const int N = ctx->N;
+  const double z0 = s[0].ZZ[s[0].snapshot];
+  auto sched = radius_schedule(&p[0], z0);
+  for (int u = 1; u < nu; ++u) {
+    auto su = radius_schedule(&p[u], s[u].ZZ[s[u].snapshot]);
+    if (su.size() != sched.size()) return set_error(ctx, RG_EINVAL, "batch units with different radius schedules");
+    for (size_t i = 0; i < su.size(); ++i)
+      if (su[i].first != sched[i].first) return set_error(ctx, RG_EINVAL, "batch units with different radii");
   }
+  std::vector<HiiConst> cs(nu);
+  for (int u = 0; u < nu; ++u)
+    if ((rc = hii_const(ctx, &p[u], s[u].ZZ[s[u].snapshot], &cs[u]))) return rc;
+  // the units' grids one after another: unit u's grid k is grid u ngu + k of the batch
+  const float* one[10];
+  int ntest = 0;
+  const int ngu = hii_sources(&p[0], &g[0], false, one, &ntest);
+  std::vector<const float*> srcs((size_t)nu * ngu);
+  for (int u = 0; u < nu; ++u) {
+    hii_sources(&p[u], &g[u], false, one, &ntest);
+    for (int k = 0; k < ngu; ++k) srcs[(size_t)u * ngu + k] = one[k];
+  }
+  const int ng = nu * ngu;
+  const size_t nc = (size_t)(N / 2 + 1) * N * N, n3 = (size_t)N * N * N;
+  const int nr = (int)sched.size();
+  int kb = ctx->radius_batch > 0 ? ctx->radius_batch : 8;
+  if (kb > KB_MAX) kb = KB_MAX;
+  if (kb > nr) kb = nr;
+  if ((rc = ensure_device(ctx, &ctx->spec, &ctx->spec_elems, nc * ng))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->work, &ctx->work_elems, nc * ng * kb))) return rc;
+  // one state byte per cell of every unit
+  if ((rc = ensure_device(ctx, &ctx->bits, &ctx->bits_elems, (n3 * nu + 3) / 4))) return rc;
+  if ((rc = ensure_device(ctx, &ctx->batch_sums, &ctx->batch_sums_elems, (size_t)32 * nu))) return rc;
+  if ((size_t)nu > ctx->h_batch_sums_elems) {
+    if (ctx->h_batch_sums) cudaFreeHost(ctx->h_batch_sums);
+    ctx->h_batch_sums = nullptr;
+    ctx->h_batch_sums_elems = 0;
+    if (cudaMallocHost((void**)&ctx->h_batch_sums, sizeof(double) * 32 * nu) != cudaSuccess)
+      return set_error(ctx, RG_ENOMEM, "pinned batch sums");
+    ctx->h_batch_sums_elems = (size_t)nu;
+  }
+  for (int g0 = 0; g0 < ng; g0 += MAXG)
+    if ((rc = fft_forward(ctx, N, srcs.data() + g0, std::min(MAXG, ng - g0), ctx->spec + nc * g0, nc,
+                          1.0 / std::pow((double)N, 3), st)))
+      return rc;
+  if ((rc = hii_windows(ctx, &p[0], sched, st))) return rc;
+  const int n2max = 3 * (N / 2) * (N / 2);
+  const int* wcut = p[0].ReionFilterType == 1 ? ctx->wcut : nullptr;
+  for (int u = 0; u < nu; ++u)
+    RG_CUDA_TRY(ctx, cudaMemsetAsync(g[u].r_bubble, 0, sizeof(float) * n3, st));
+  double* partials = ensure_partials(ctx, (size_t)N * N * HII_NSUM);
+  if (!partials) return set_error(ctx, RG_ENOMEM, "partials");
+  std::vector<HiiState> hs(nu);
+  for (int u = 0; u < nu; ++u)
+    hs[u] = hii_state(&p[u], &g[u], reinterpret_cast<uint8_t*>(ctx->bits) + n3 * u, partials);
+
+  if ((rc = xy_ctrl_reset(ctx, (size_t)(N / 2 + 1) * kb, st))) return rc;
+  for (int r0 = 0; r0 < nr; r0 += kb) {
+    const int cnt = std::min(kb, nr - r0);
+    const bool fin = (r0 + cnt == nr);
+    const int unf = fin ? cnt - 1 : -1;
+    // the windowed inverse x/y passes of every unit's grids in one launch; unit u's block of
+    // the work buffer is [radius][its grids], as a single snapshot's
+    if ((rc = inverse_xy(ctx, N, ctx->spec, ng, ngu, ctx->work, nc, cnt, ctx->wtab + (size_t)r0 * (n2max + 1),
+                         n2max + 1, unf, st, wcut ? wcut + r0 : nullptr)))
+      return rc;
+    for (int u = 0; u < nu; ++u) {
+      HiiBatch bt;
+      hii_batch_radii(&p[u], s[u].ZZ[s[u].snapshot], sched, r0, cnt, ntest, &bt);
+      int nblocks = 0;
+      if ((rc = hii_z(ctx, N, ctx->work + (size_t)u * cnt * ngu * nc, nc, ntest, bt, cs[u], hs[u], fin, st, &nblocks)))
+        return rc;
+      if (fin && (rc = reduce_partials(ctx, partials, nblocks, HII_NSUM, ctx->batch_sums + 32 * u, st))) return rc;
+    }
+  }
+  RG_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_batch_sums, ctx->batch_sums, sizeof(double) * 32 * nu,
+                                   cudaMemcpyDeviceToHost, st));
+  RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  prof_resolve(ctx);
+  if ((rc = xy_ctrl_check(ctx, st))) return rc;
+  for (int u = 0; u < nu; ++u) hii_outputs(&p[u], nr, ctx->h_batch_sums + 32 * u, &out[u]);
   return RG_OK;
 }
 

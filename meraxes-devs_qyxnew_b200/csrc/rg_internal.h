@@ -139,6 +139,11 @@ int stage_record(rg_context* ctx, size_t i, cudaStream_t st, cudaEvent_t* out);
 // The excursion-set step on device grids (rg_hii.cu).
 int hii_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const rg_grids* g, rg_hii_scalars* out,
                  const Staging* stg = nullptr);
+// find_HII_bubbles for nu snapshots of this size with the same radii, device grids, fused mode:
+// the forward transforms and every radius batch's x/y passes of all of them in shared launches,
+// the z passes per snapshot, one host synchronisation.
+int hii_batch(rg_context* ctx, int nu, const rg_params* p, const rg_snapshot* s, const rg_grids* g,
+              rg_hii_scalars* out);
 // The spin-temperature step on device grids (rg_ts.cu).  With src_host, the sfr /
 // xray_luminosity grids and their histories are read from those HOST arrays instead of g, and
 // only the history slots the shells use are copied to the device (on the copy stream, one
@@ -215,6 +220,10 @@ struct rg_context {
   size_t partials_elems = 0;
   double* d_sums = nullptr;      // reduced sums
   double* h_sums = nullptr;      // pinned host copy
+  double* batch_sums = nullptr;  // rg_find_HII_bubbles_batch: reduced sums per snapshot [unit][32]
+  size_t batch_sums_elems = 0;
+  double* h_batch_sums = nullptr;   // their pinned host copy (h_batch_sums_elems snapshots)
+  size_t h_batch_sums_elems = 0;
   // device grids owned by the context (rg_alloc_grids / host entry points)
   std::vector<void*> owned;
   rg_grids dev_grids{};

@@ -83,17 +83,32 @@ __device__ __forceinline__ void xy_wait(const XYSched& s, int job) {
   atomicExch(s.err, 1u);
 }
 
+// The fused pass's radix plans: the default plans, except 512 = 8 x 16 x 4 over 32 threads a line
+// (16 values a thread), which measured faster here than 8 x 8 x 8 over 64 threads (77.2 against
+// 81.3 ms for the 61 radii of a 512^3 snapshot; 16 x 16 x 2 took 78.5 ms, and 16 columns an item
+// instead of 8 took 85-87 ms)
+template <int N>
+struct PlanXY : Plan<N> {};
+template <>
+struct PlanXY<512> {
+  static constexpr int NN = 512;
+  static constexpr int T = 32;
+  static constexpr int R[] = {8, 16, 4};
+  static constexpr int S = 3;
+};
 template <int N>
 struct XYF {
-  static constexpr int T = Cfg<N>::T;
-  static constexpr int V = Cfg<N>::V;
+  using PL = PlanXY<N>;
+  static constexpr int T = PL::T;
+  static constexpr int V = N / T;
   static constexpr int B = Cfg<N>::BX;   // columns per X item, lines per Y item
+  static constexpr int MINB = N != 512 ? x_pass_minb<N>() : 2;
   static constexpr int NTH = T * B;
   static constexpr int M = N / B;
   static constexpr int XROWS = N <= 256 ? N : N / 2;   // x rows per tensor box (box dimensions <= 256)
   static constexpr int NXB = N / XROWS;
   // a buffer: an X tile [x][B columns], then its exchange buffer; or a Y item's exchange buffer
-  static constexpr int TB = round_up(cmax(cmax(line_buf<N, B>(), B * Cfg<N>::PITCH_P), N * B), 16);
+  static constexpr int TB = round_up(cmax(cmax(line_buf_r0<N, PL::R[0], B>(), B * Cfg<N>::PITCH_P), N * B), 16);
   static constexpr int ZB = 2;
   static constexpr uint32_t TX = (uint32_t)(N * B * sizeof(cf));
   static constexpr size_t smem() { return 128 + sizeof(cf) * ((size_t)ZB * TB + N) + sizeof(uint64_t) * ZB; }
@@ -121,9 +136,10 @@ __device__ __forceinline__ void xy_signal(uint32_t* p) {
 // The X input of grid g is W(k) * spectrum_g(k); the spectra are the tensor `smap` (floats, y
 // innermost, then x, then kz of grid g at g (N/2 + 1) + kz).
 template <int N, class Op>
-__global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
+__global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
     k_xy_fused(XYSched sch, Op op, const __grid_constant__ CUtensorMap smap, const cf* __restrict__ g_tw) {
   using F = XYF<N>;
+  using PL = typename F::PL;
   constexpr int T = F::T, B = F::B, V = F::V, TB = F::TB, NZ = N / 2 + 1;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sm = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
@@ -136,7 +152,7 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
     for (int b = 0; b < F::ZB; ++b) mbar_init(&bars[b], 1);
     mbar_init_fence();
   }
-  load_twiddles<N>(s_tw, g_tw);
+  load_twiddles_p<PL>(s_tw, g_tw);
   if (threadIdx.x == 0) {
     s_item[0] = (int)atomicAdd(sch.ctr, 1u);
     s_pref[0] = 0;
@@ -190,7 +206,7 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
         const int ny = y > N / 2 ? y - N : y;
 #pragma unroll
         for (int sl = 0; sl < V; ++sl) {
-          const int p = stage0_pos<N>(t, sl);
+          const int p = stage0_pos<PL>(t, sl);
           const int nx = p > N / 2 ? p - N : p;
           const int n2 = nx * nx + ny * ny + kz * kz;
           wv[sl] = cut >= -1 ? (n2 <= cut ? 1.f : 0.f) : __ldg(wr + n2);
@@ -211,13 +227,14 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
         if (!mbar_wait(&bars[b], (xu >> 1) & 1u, 1 << 22)) waited = false;
         cf* tile = bufs + b * TB;
         cf* dst = op.out(r, g);
-        line_fft<N, true>(
+        line_fft_p<PL, true>(
             t, tile, s_tw,
             [&](int p, int sl) {
               const cf v = tile[p * B + bcol];
               return cf{v.x * wv[sl], v.y * wv[sl]};
             },
-            [&](int p) { return line_addr<N, B>(p, bcol); }, [&](int p, cf v) { dst[col + (size_t)p * N] = v; });
+            [&](int p) { return line_addr_r0<PL::R[0], B>(p, bcol); },
+            [&](int p, cf v, int) { dst[col + (size_t)p * N] = v; });
         fence_proxy_async_smem();
         __syncthreads();   // every store of the unit is issued; its buffer may be refilled
       }
@@ -229,9 +246,9 @@ __global__ void __launch_bounds__(XYF<N>::NTH, (x_pass_minb<N>()))
       const size_t row = plane + (size_t)(k * B + b) * N;
       for (int g = 0; g < ng; ++g) {
         cf* line = op.out(r, g) + row;
-        line_fft<N, true>(
+        line_fft_p<PL, true>(
             t, bufs, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return pos_addr<N>(b, p); },
-            [&](int p, cf v) { line[p] = v; });
+            [&](int p, cf v, int) { line[p] = v; });
       }
       fence_proxy_async_smem();   // the exchange buffer is a tile buffer of later X items
     }

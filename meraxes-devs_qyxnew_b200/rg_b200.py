@@ -15,6 +15,7 @@ TABLES_DIR = os.path.join(HERE, "data", "21cmFAST-tables")
 
 RG_OK, RG_EINVAL, RG_ENOMEM, RG_ECUDA, RG_EUNSUPPORTED, RG_ETABLE, RG_ENODEV, RG_ETIMEDOUT = range(8)
 RG_MODE_FUSED, RG_MODE_PLAIN = 0, 1
+RG_DFT_FP32, RG_DFT_TC_BF16X3 = 0, 1
 
 
 class rg_params(C.Structure):
@@ -116,6 +117,9 @@ _SIGS = {
     "rg_set_radius_batch": (C.c_int, [C.c_void_p, C.c_int]),
     "rg_debug_set_wait_limits": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "rg_push_histories": (C.c_int, [C.c_void_p, _P(rg_params), _P(rg_grids)]),
+    "rg_dft_y_pass": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "rg_find_HII_bubbles_batch": (C.c_int, [C.c_void_p, C.c_int, _P(rg_params), _P(rg_snapshot), _P(rg_grids),
+                                            _P(rg_hii_scalars)]),
     "rg_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "rg_last_error": (C.c_char_p, [C.c_void_p]),
     "rg_status_string": (C.c_char_p, [C.c_int]),
@@ -278,6 +282,15 @@ class Context:
 
     def call(self, name, *args):
         check(self.h, getattr(self.lib, name)(self.h, *args))
+
+    def find_hii_batch(self, ps, ss, gs):
+        """rg_find_HII_bubbles_batch over the units (params, snapshots, grids); returns their
+        rg_hii_scalars.  The snapshots' redshift arrays stay owned by the rg_snapshot objects."""
+        n = len(ps)
+        pa, sa, ga = (rg_params * n)(*ps), (rg_snapshot * n)(*ss), (rg_grids * n)(*gs)
+        oa = (rg_hii_scalars * n)()
+        self.call("rg_find_HII_bubbles_batch", n, pa, sa, ga, oa)
+        return [rg_hii_scalars.from_buffer_copy(oa[i]) for i in range(n)]
 
     def power_spectrum(self, p: rg_params, delta_T_ptr: int, host: bool = False, max_bins: int = 64):
         """Compute_PS of delta_T (a device pointer, or a host pointer with host=True): returns
