@@ -524,7 +524,12 @@ def time_recombinations(wk, ctx, torch, stream, dev):
     n = wk.n
     npad, nreal = n * n * 2 * (n // 2 + 1), n ** 3
     ctx.set_recombination_tables(*wl.rec_stand_in_tables())
-    extra = {"Gamma12": torch.zeros(nreal, device=dev), "N_rec": torch.zeros(npad, device=dev),
+    # recombinations accumulated over earlier snapshots (N_rec up to 0.4 per baryon) and an
+    # ionising background, so the barrier's 1 + N_rec term and the recombination closing pass see
+    # non-zero state
+    gen = torch.Generator(device=dev).manual_seed(7)
+    extra = {"Gamma12": torch.rand(nreal, device=dev, generator=gen) * 0.5,
+             "N_rec": torch.rand(npad, device=dev, generator=gen) * 0.4,
              "residual_xH": torch.zeros(nreal, device=dev), "clumping_factor": torch.zeros(nreal, device=dev),
              "t_resp": torch.full((nreal,), 1e30, device=dev)}
     gr = rg.rg_grids.from_buffer_copy(wk.g)

@@ -254,14 +254,12 @@ template <bool INV>
 int launch_tc(rg_context* ctx, cf* spec, size_t stride, int ng, cudaStream_t st) {
   auto kern = k_pass_y_tc<INV>;
   RG_CUDA_TRY(ctx, set_smem(kern, TC_SMEM));
-  int per_sm = 0;
-  RG_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TC_NT, TC_SMEM));
-  // tensor memory: every resident block holds TC_COLS of the SM's 512 columns; more resident
-  // blocks than that would wait in tcgen05.alloc
-  if (per_sm < 1) return set_error(ctx, RG_ECUDA, "tensor-core y pass: no block fits an SM");
-  if (per_sm * TC_COLS > 512) per_sm = 512 / TC_COLS;
+  // persistent blocks: TC_BLOCKS_PER_SM per SM (shared memory allows five; tensor memory, 32 of
+  // the SM's 512 columns a block, sixteen).  Blocks are independent, so any that do not fit at
+  // once simply start later.
+  static_assert(TC_BLOCKS_PER_SM * TC_COLS <= 512, "tensor memory columns per SM");
   const int ntiles = ng * ((TC_N / 2 + 1) * TC_N / TC_L);
-  const int grid = std::min(ntiles, per_sm * ctx->num_sms);
+  const int grid = std::min(ntiles, TC_BLOCKS_PER_SM * ctx->num_sms);
   int rc = xy_ctrl_reset(ctx, 0, st);
   if (rc) return rc;
   prof_begin(ctx, "dft_y_tc_bf16x3", st);
@@ -274,16 +272,12 @@ int launch_tc(rg_context* ctx, cf* spec, size_t stride, int ng, cudaStream_t st)
 template <bool INV>
 int launch_fp32(rg_context* ctx, cf* spec, size_t stride, int ng, cudaStream_t st) {
   constexpr int N = TC_N;
-  using C = Cfg<N>;
   const cf* tw;
   int rc = twiddles_for(ctx, N, &tw);
   if (rc) return rc;
-  const size_t smem = sizeof(cf) * (N + (size_t)C::BY * C::PITCH_P);
-  RG_CUDA_TRY(ctx, set_smem(k_pass_y<N, INV>, smem));
   prof_begin(ctx, "dft_y_fp32", st);
-  k_pass_y<N, INV><<<dim3(N / C::BY, C::NZ, ng), C::T * C::BY, smem, st>>>(spec, stride, tw);
+  RG_CUDA_TRY(ctx, (launch_pass_y<N, INV>(spec, stride, ng, tw, st)));
   prof_end(ctx, ng * 16.0 * (double)stride, st);
-  RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 

@@ -267,14 +267,22 @@ __device__ __forceinline__ void stage_emit(const cf* v, int t, Put&& put) {
   }
 }
 
-template <class PL, int s, bool INV, class Addr, class Store>
+// WS: every line's threads are lanes of one warp and its exchange buffer region is its own, so
+// a warp barrier orders the exchange; otherwise a block barrier
+template <bool WS>
+__device__ __forceinline__ void exchange_sync() {
+  if constexpr (WS) __syncwarp();
+  else __syncthreads();
+}
+
+template <class PL, int s, bool INV, bool WS = false, class Addr, class Store>
 __device__ __forceinline__ void stages_from(cf* v, int t, cf* xbuf, Addr&& addr, const cf* tw, Store&& store) {
   if constexpr (s + 1 < PL::S) {
-    __syncthreads();  // every thread is done reading xbuf
+    exchange_sync<WS>();  // every thread is done reading xbuf
     stage_emit<PL, s>(v, t, [&](int p, cf x, int) { xbuf[addr(p)] = x; });
-    __syncthreads();
+    exchange_sync<WS>();
     stage_compute<PL, s + 1, INV>(v, t, tw, [&](int p, int) { return xbuf[addr(p)]; });
-    stages_from<PL, s + 1, INV>(v, t, xbuf, addr, tw, store);
+    stages_from<PL, s + 1, INV, WS>(v, t, xbuf, addr, tw, store);
   } else {
     stage_emit<PL, s>(v, t, store);
   }
@@ -295,14 +303,17 @@ __device__ __forceinline__ int last_pos(int t, int slot) {
 //                          (stage0_pos<PL>(t, slot) == p)
 //   addr(p)             -> index into xbuf of position p of this thread's line (exchange buffer)
 //   store(p, val, slot) <- output element at position p (last_pos<PL>(t, slot) == p)
-// Every thread of the block must call it (it contains block barriers when S > 1).
-template <class PL, bool INV, class Load, class Addr, class Store>
+// Every thread of the block must call it (it contains block barriers when S > 1, unless WS).
+//   WS: the line's threads are lanes of one warp (T <= 32, consecutive lanes) and addr() maps
+//   each line into a region of xbuf no other line uses: warp barriers instead of block barriers.
+template <class PL, bool INV, bool WS = false, class Load, class Addr, class Store>
 __device__ __forceinline__ void line_fft_p(int t, cf* xbuf, const cf* tw, Load&& load, Addr&& addr, Store&& store) {
   static_assert(plan_product<PL>() == PL::NN, "radix plan does not multiply to N");
+  static_assert(!WS || (PL::T <= 32 && 32 % PL::T == 0), "warp barriers need a line within a warp");
   constexpr int V = PL::NN / PL::T;
   cf v[V];
   stage_compute<PL, 0, INV>(v, t, tw, load);
-  stages_from<PL, 0, INV>(v, t, xbuf, addr, tw, store);
+  stages_from<PL, 0, INV, WS>(v, t, xbuf, addr, tw, store);
 }
 
 // line_fft with the default plan; store(p, val) without the slot

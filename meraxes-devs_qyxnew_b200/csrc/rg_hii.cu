@@ -635,8 +635,6 @@ static cudaError_t prep(K kernel, size_t smem) {
 template <int N>
 constexpr size_t smem_x() { return sizeof(cf) * (N + (size_t)line_buf<N, Cfg<N>::BX>()); }
 template <int N>
-constexpr size_t smem_y() { return sizeof(cf) * (N + (size_t)Cfg<N>::BY * Cfg<N>::PITCH_P); }
-template <int N>
 constexpr size_t smem_fz() { return sizeof(cf) * (N + 2 * (size_t)Cfg<N>::QF * Cfg<N>::PITCH_P); }
 
 template <int N>
@@ -654,11 +652,9 @@ int launch_forward(rg_context* ctx, const float* const* d_real, int ng, cf* spec
   k_fwd_z<N><<<dim3(N / (2 * C::QF), N, ng), C::T * C::QF, smem_fz<N>(), st>>>(src, spec, stride, tw);
   prof_end(ctx, ng * (4.0 * N * N * N + 8.0 * nzc), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
-  RG_CUDA_TRY(ctx, prep(k_pass_y<N, false>, smem_y<N>()));
   prof_begin(ctx, "fwd_y_c2c", st);
-  k_pass_y<N, false><<<dim3(N / C::BY, C::NZ, ng), C::T * C::BY, smem_y<N>(), st>>>(spec, stride, tw);
+  RG_CUDA_TRY(ctx, (launch_pass_y<N, false>(spec, stride, ng, tw, st)));
   prof_end(ctx, ng * 16.0 * nzc, st);
-  RG_CUDA_TRY(ctx, cudaGetLastError());
   RG_CUDA_TRY(ctx, prep(k_pass_x_fwd<N>, smem_x<N>()));
   prof_begin(ctx, "fwd_x_c2c", st);
   k_pass_x_fwd<N><<<dim3(N / C::BX, C::NZ, ng), C::T * C::BX, smem_x<N>(), st>>>(spec, stride, tw, (float)scale);
@@ -976,11 +972,9 @@ int launch_inverse_xy(rg_context* ctx, const cf* spec, int ng, int ngu, cf* work
                                                                         unfiltered, tw);
   prof_end(ctx, ng * 8.0 * nzc * (1 + nr), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
-  RG_CUDA_TRY(ctx, prep(k_pass_y<N, true>, smem_y<N>()));
   prof_begin(ctx, "inv_y_c2c", st);
-  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, ng * nr), C::T * C::BY, smem_y<N>(), st>>>(work, stride, tw);
+  RG_CUDA_TRY(ctx, (launch_pass_y<N, true>(work, stride, ng * nr, tw, st)));
   prof_end(ctx, ng * nr * 16.0 * nzc, st);
-  RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 

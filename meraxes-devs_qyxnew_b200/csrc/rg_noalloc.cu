@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<
 template <int N>
 constexpr size_t na_smem_fz() { return sizeof(cf) * (N + 2 * (size_t)Cfg<N>::QF * Cfg<N>::PITCH_P); }
 template <int N>
-constexpr size_t na_smem_y() { return sizeof(cf) * (N + (size_t)Cfg<N>::BY * Cfg<N>::PITCH_P); }
+constexpr size_t na_smem_y() { return YCfg<N>::smem(); }
 template <int N>
 constexpr size_t na_smem_x() { return sizeof(cf) * (N + (size_t)line_buf<N, Cfg<N>::BX>()); }
 
@@ -147,13 +147,13 @@ cudaError_t na_roundtrip(unsigned char* base, const float* in, float* out, doubl
   GridPtrs srcs{};
   srcs.p[0] = in;
   k_fwd_z<N><<<dim3(N / (2 * C::QF), N, 1), C::T * C::QF, na_smem_fz<N>(), st>>>(srcs, spec, nc, tw);
-  k_pass_y<N, false><<<dim3(N / C::BY, C::NZ, 1), C::T * C::BY, na_smem_y<N>(), st>>>(spec, nc, tw);
+  k_pass_y<N, false><<<dim3(N / YCfg<N>::BY, C::NZ, 1), YCfg<N>::NTH, na_smem_y<N>(), st>>>(spec, nc, tw);
   k_pass_x_fwd<N><<<dim3(N / C::BX, C::NZ, 1), C::T * C::BX, na_smem_x<N>(), st>>>(
       spec, nc, tw, (float)(1.0 / ((double)N * N * N)));
   // filter_type < 0: the window is 1 everywhere (no filter)
   k_na_inv_x<N><<<dim3(N / C::BX, C::NZ), C::T * C::BX, na_smem_x<N>(), st>>>(spec, work, tw, 2.0 * M_PI / box, R,
                                                                                ftype);
-  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, 1), C::T * C::BY, na_smem_y<N>(), st>>>(work, nc, tw);
+  k_pass_y<N, true><<<dim3(N / YCfg<N>::BY, C::NZ, 1), YCfg<N>::NTH, na_smem_y<N>(), st>>>(work, nc, tw);
   k_inv_z_padded<N><<<dim3(N / (2 * C::QZ), N), C::T * C::QZ, zfront_smem_bytes<N>(1), st>>>(work, tw, out);
   return cudaGetLastError();
 }

@@ -131,9 +131,9 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF, RG_MINB(Cfg<N>::T* Cfg<
   load_twiddles<N>(s_tw, g_tw);
   __syncthreads();
   const float* r0 = src + ((size_t)x * N + y0 + 2 * q) * PADW;
-  line_fft<N, false>(
+  line_fft_p<Plan<N>, false, (T <= 32)>(   // warp barriers when a line fits a warp (its rows are its own)
       t, xbuf, s_tw, [&](int p, int) { return cf{__ldg(r0 + p), __ldg(r0 + PADW + p)}; },
-      [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v) { zbuf[pos_addr<N>(q, p)] = v; });
+      [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v, int) { zbuf[pos_addr<N>(q, p)] = v; });
   __syncthreads();
   // split Z = X(y) + i X(y+1) and store S[k][x][y0 .. y0 + 2Q)
   for (int i = threadIdx.x; i < NZ * 2 * Q; i += T * Q) {
@@ -151,11 +151,36 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF, RG_MINB(Cfg<N>::T* Cfg<
   }
 }
 
-// y pass over grids base + z * stride (z = blockIdx.z), in place
+// Plans of at most 32 threads a line, for passes whose lines may then be warp-local: the default
+// plans, except 512 = 8 x 16 x 4 over 32 threads (16 values a thread)
+template <int N>
+struct PlanW : Plan<N> {};
+template <>
+struct PlanW<512> {
+  static constexpr int NN = 512;
+  static constexpr int T = 32;
+  static constexpr int R[] = {8, 16, 4};
+  static constexpr int S = 3;
+};
+
+// the y pass's launch shape: BY lines of T threads per block
+template <int N>
+struct YCfg {
+  using PL = PlanW<N>;
+  static constexpr int T = PL::T;
+  static constexpr int BY = pow2_div(N, cmax(256 / T, 1));
+  static constexpr int NTH = T * BY;
+  static constexpr size_t smem() { return sizeof(cf) * (N + (size_t)BY * Cfg<N>::PITCH_P); }
+};
+
+// y pass over grids base + z * stride (z = blockIdx.z), in place.  A line's T <= 32 threads are
+// consecutive lanes of one warp and its exchange row is its own: warp barriers.
 template <int N, bool INV>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BY, RG_MINB(Cfg<N>::T* Cfg<N>::BY))
+__global__ void __launch_bounds__(YCfg<N>::NTH, RG_MINB(YCfg<N>::NTH))
     k_pass_y(cf* __restrict__ base, size_t stride, const cf* __restrict__ g_tw) {
-  constexpr int T = Cfg<N>::T, B = Cfg<N>::BY;
+  using Y = YCfg<N>;
+  using PL = typename Y::PL;
+  constexpr int T = Y::T, B = Y::BY;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
   cf* xbuf = smem + N;
@@ -163,12 +188,22 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BY, RG_MINB(Cfg<N>::T* Cfg<
   const int kz = blockIdx.y;
   const int x0 = blockIdx.x * B;
   const int t = threadIdx.x % T, b = threadIdx.x / T;
-  load_twiddles<N>(s_tw, g_tw);
+  load_twiddles_p<PL>(s_tw, g_tw);
   __syncthreads();
   cf* line = g + ((size_t)kz * N + x0 + b) * N;
-  line_fft<N, INV>(
+  line_fft_p<PL, INV, true>(
       t, xbuf, s_tw, [&](int p, int) { return line[p]; }, [&](int p) { return pos_addr<N>(b, p); },
-      [&](int p, cf v) { line[p] = v; });
+      [&](int p, cf v, int) { line[p] = v; });
+}
+
+// the y pass over ng grids at base + g * stride
+template <int N, bool INV>
+inline cudaError_t launch_pass_y(cf* base, size_t stride, int ng, const cf* tw, cudaStream_t st) {
+  using Y = YCfg<N>;
+  cudaError_t e = cudaFuncSetAttribute(k_pass_y<N, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Y::smem());
+  if (e != cudaSuccess) return e;
+  k_pass_y<N, INV><<<dim3(N / Y::BY, Cfg<N>::NZ, ng), Y::NTH, Y::smem(), st>>>(base, stride, tw);
+  return cudaGetLastError();
 }
 
 // forward x pass over grids base + z * stride, in place, scaled on store

@@ -731,12 +731,9 @@ static int launch_ts_xy(rg_context* ctx, const cf* spec, cf* work_base, size_t s
   for (int r = 0; r < bt.nr; ++r) src_reads += bt.nk[r];
   prof_end(ctx, bt.ng * 8.0 * nzc * (src_reads + bt.nr), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
-  const size_t smy = sizeof(cf) * (N + (size_t)C::BY * C::PITCH_P);
-  RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_pass_y<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy));
   prof_begin(ctx, "ts_y_c2c", st);
-  k_pass_y<N, true><<<dim3(N / C::BY, C::NZ, bt.ng * bt.nr), C::T * C::BY, smy, st>>>(work_base, stride, tw);
+  RG_CUDA_TRY(ctx, (launch_pass_y<N, true>(work_base, stride, bt.ng * bt.nr, tw, st)));
   prof_end(ctx, bt.ng * bt.nr * 16.0 * nzc, st);
-  RG_CUDA_TRY(ctx, cudaGetLastError());
   return RG_OK;
 }
 

@@ -83,22 +83,12 @@ __device__ __forceinline__ void xy_wait(const XYSched& s, int job) {
   atomicExch(s.err, 1u);
 }
 
-// The fused pass's radix plans: the default plans, except 512 = 8 x 16 x 4 over 32 threads a line
-// (16 values a thread), which measured faster here than 8 x 8 x 8 over 64 threads (77.2 against
-// 81.3 ms for the 61 radii of a 512^3 snapshot; 16 x 16 x 2 took 78.5 ms, and 16 columns an item
-// instead of 8 took 85-87 ms)
-template <int N>
-struct PlanXY : Plan<N> {};
-template <>
-struct PlanXY<512> {
-  static constexpr int NN = 512;
-  static constexpr int T = 32;
-  static constexpr int R[] = {8, 16, 4};
-  static constexpr int S = 3;
-};
+// The fused pass's plans (PlanW): at 512, 8 x 16 x 4 over 32 threads a line measured faster than
+// 8 x 8 x 8 over 64 (77.2 against 81.3 ms for the 61 radii of a 512^3 snapshot; 16 x 16 x 2 took
+// 78.5 ms, and 16 columns an item instead of 8 took 85-87 ms), and its Y lines are warp-local.
 template <int N>
 struct XYF {
-  using PL = PlanXY<N>;
+  using PL = PlanW<N>;
   static constexpr int T = PL::T;
   static constexpr int V = N / T;
   static constexpr int B = Cfg<N>::BX;   // columns per X item, lines per Y item
@@ -244,9 +234,10 @@ __global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
       __syncthreads();
       const int t = threadIdx.x % T, b = threadIdx.x / T;
       const size_t row = plane + (size_t)(k * B + b) * N;
+      // a line's T <= 32 threads are consecutive lanes of one warp, its exchange rows its own
       for (int g = 0; g < ng; ++g) {
         cf* line = op.out(r, g) + row;
-        line_fft_p<PL, true>(
+        line_fft_p<PL, true, (T <= 32)>(
             t, bufs, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return pos_addr<N>(b, p); },
             [&](int p, cf v, int) { line[p] = v; });
       }

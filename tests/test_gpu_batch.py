@@ -42,7 +42,7 @@ def fresh(units, torch):
 def test_batch_equals_one_at_a_time(n, spin, kb):
     import torch
     units = [(n, float(n), z, eff, 100 + i, spin) for i, (z, eff) in
-             enumerate([(12.0, 3000.0), (9.5, 60.0), (8.0, 4000.0), (7.0, 900.0)])]
+             enumerate([(12.0, 3000.0), (9.5, 60.0), (8.0, 40000.0), (7.0, 900.0)])]
     ctx = rg.Context(n)
     ctx.call("rg_set_radius_batch", kb)
     one = fresh(units, torch)
