@@ -634,8 +634,6 @@ static cudaError_t prep(K kernel, size_t smem) {
 
 template <int N>
 constexpr size_t smem_x() { return sizeof(cf) * (N + (size_t)line_buf<N, Cfg<N>::BX>()); }
-template <int N>
-constexpr size_t smem_fz() { return sizeof(cf) * (N + 2 * (size_t)Cfg<N>::QF * Cfg<N>::PITCH_P); }
 
 template <int N>
 int launch_forward(rg_context* ctx, const float* const* d_real, int ng, cf* spec, size_t stride, double scale,
@@ -647,9 +645,10 @@ int launch_forward(rg_context* ctx, const float* const* d_real, int ng, cf* spec
   GridPtrs src{};
   for (int g = 0; g < ng; ++g) src.p[g] = d_real[g];
   const double nzc = (double)C::NZ * N * N;
-  RG_CUDA_TRY(ctx, prep(k_fwd_z<N>, smem_fz<N>()));
+  using ZF = ZFCfg<N>;
+  RG_CUDA_TRY(ctx, prep(k_fwd_z<N>, ZF::smem()));
   prof_begin(ctx, "fwd_z_r2c", st);
-  k_fwd_z<N><<<dim3(N / (2 * C::QF), N, ng), C::T * C::QF, smem_fz<N>(), st>>>(src, spec, stride, tw);
+  k_fwd_z<N><<<dim3(N / (2 * ZF::QF), N, ng), ZF::NTH, ZF::smem(), st>>>(src, spec, stride, tw);
   prof_end(ctx, ng * (4.0 * N * N * N + 8.0 * nzc), st);
   RG_CUDA_TRY(ctx, cudaGetLastError());
   prof_begin(ctx, "fwd_y_c2c", st);

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::BX, RG_MINB(Cfg<N>::T* Cfg<
 }
 
 template <int N>
-constexpr size_t na_smem_fz() { return sizeof(cf) * (N + 2 * (size_t)Cfg<N>::QF * Cfg<N>::PITCH_P); }
+constexpr size_t na_smem_fz() { return ZFCfg<N>::smem(); }
 template <int N>
 constexpr size_t na_smem_y() { return YCfg<N>::smem(); }
 template <int N>
@@ -146,7 +146,7 @@ cudaError_t na_roundtrip(unsigned char* base, const float* in, float* out, doubl
   k_na_twiddles<<<1, N, 0, st>>>(tw, N);
   GridPtrs srcs{};
   srcs.p[0] = in;
-  k_fwd_z<N><<<dim3(N / (2 * C::QF), N, 1), C::T * C::QF, na_smem_fz<N>(), st>>>(srcs, spec, nc, tw);
+  k_fwd_z<N><<<dim3(N / (2 * ZFCfg<N>::QF), N, 1), ZFCfg<N>::NTH, na_smem_fz<N>(), st>>>(srcs, spec, nc, tw);
   k_pass_y<N, false><<<dim3(N / YCfg<N>::BY, C::NZ, 1), YCfg<N>::NTH, na_smem_y<N>(), st>>>(spec, nc, tw);
   k_pass_x_fwd<N><<<dim3(N / C::BX, C::NZ, 1), C::T * C::BX, na_smem_x<N>(), st>>>(
       spec, nc, tw, (float)(1.0 / ((double)N * N * N)));

@@ -70,6 +70,18 @@ struct Cfg {
   static constexpr int RT_PITCH = N + 1;  // real row pitch (floats) in zfront
 };
 
+// Plans of at most 32 threads a line, for passes whose lines may then be warp-local: the default
+// plans, except 512 = 8 x 16 x 4 over 32 threads (16 values a thread)
+template <int N>
+struct PlanW : Plan<N> {};
+template <>
+struct PlanW<512> {
+  static constexpr int NN = 512;
+  static constexpr int T = 32;
+  static constexpr int R[] = {8, 16, 4};
+  static constexpr int S = 3;
+};
+
 // minimum resident blocks of the windowed inverse x passes: with radix-8 plans two blocks of 512
 // threads (at most 64 registers); otherwise the general cap
 template <int N>
@@ -115,10 +127,21 @@ __host__ __device__ constexpr int line_buf_r0() {
 
 // ---------------------------------------------------------------------------
 
+// the forward z pass's launch shape: QF row pairs per block, one line of T threads each
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF, RG_MINB(Cfg<N>::T* Cfg<N>::QF))
+struct ZFCfg {
+  using PL = PlanW<N>;
+  static constexpr int T = PL::T;
+  static constexpr int QF = pow2_div(N / 2, cmax(256 / T, 1));
+  static constexpr int NTH = T * QF;
+  static constexpr size_t smem() { return sizeof(cf) * (N + 2 * (size_t)QF * Cfg<N>::PITCH_P); }
+};
+
+template <int N>
+__global__ void __launch_bounds__(ZFCfg<N>::NTH, RG_MINB(ZFCfg<N>::NTH))
     k_fwd_z(GridPtrs srcs, cf* __restrict__ dst_base, size_t dst_stride, const cf* __restrict__ g_tw) {
-  constexpr int T = Cfg<N>::T, Q = Cfg<N>::QF, NZ = Cfg<N>::NZ, PADW = Cfg<N>::PADW, PI = Cfg<N>::PITCH_P;
+  using PL = typename ZFCfg<N>::PL;
+  constexpr int T = ZFCfg<N>::T, Q = ZFCfg<N>::QF, NZ = Cfg<N>::NZ, PADW = Cfg<N>::PADW, PI = Cfg<N>::PITCH_P;
   extern __shared__ cf smem[];
   cf* s_tw = smem;
   cf* xbuf = smem + N;
@@ -128,10 +151,10 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF, RG_MINB(Cfg<N>::T* Cfg<
   const int x = blockIdx.y;
   const int y0 = blockIdx.x * 2 * Q;
   const int t = threadIdx.x % T, q = threadIdx.x / T;
-  load_twiddles<N>(s_tw, g_tw);
+  load_twiddles_p<PL>(s_tw, g_tw);
   __syncthreads();
   const float* r0 = src + ((size_t)x * N + y0 + 2 * q) * PADW;
-  line_fft_p<Plan<N>, false, (T <= 32)>(   // warp barriers when a line fits a warp (its rows are its own)
+  line_fft_p<PL, false, true>(   // warp barriers: a line's threads are one warp's lanes, its rows its own
       t, xbuf, s_tw, [&](int p, int) { return cf{__ldg(r0 + p), __ldg(r0 + PADW + p)}; },
       [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v, int) { zbuf[pos_addr<N>(q, p)] = v; });
   __syncthreads();
@@ -150,18 +173,6 @@ __global__ void __launch_bounds__(Cfg<N>::T* Cfg<N>::QF, RG_MINB(Cfg<N>::T* Cfg<
     dst[((size_t)k * N + x) * N + y0 + yy] = out;
   }
 }
-
-// Plans of at most 32 threads a line, for passes whose lines may then be warp-local: the default
-// plans, except 512 = 8 x 16 x 4 over 32 threads (16 values a thread)
-template <int N>
-struct PlanW : Plan<N> {};
-template <>
-struct PlanW<512> {
-  static constexpr int NN = 512;
-  static constexpr int T = 32;
-  static constexpr int R[] = {8, 16, 4};
-  static constexpr int S = 3;
-};
 
 // the y pass's launch shape: BY lines of T threads per block
 template <int N>
