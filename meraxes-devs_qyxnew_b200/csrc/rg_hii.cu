@@ -1190,7 +1190,9 @@ int xy_ctrl_check(rg_context* ctx, cudaStream_t st) {
   uint32_t err = 0;
   RG_CUDA_TRY(ctx, cudaMemcpyAsync(&err, ctx->xy_ctrl, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-  if (err) return set_error(ctx, RG_ETIMEDOUT, "fused x/y pass: a wait for the x pass of a plane ran out");
+  if (err)
+    return set_error(ctx, RG_ETIMEDOUT,
+                     "a bounded device wait ran out (the fused x/y pass's wait for a plane, or a tensor tile's)");
   return RG_OK;
 }
 
