@@ -39,10 +39,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait for phase `parity` of the barrier to complete
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for phase `parity` of the barrier to complete: at most `limit` polls and at most
+// half a second (a poll may itself suspend the thread for a while)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit) {
-  for (int i = 0; i < limit; ++i)
+  const uint64_t t0 = global_ns();
+  for (int i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255 && global_ns() - t0 > 500000000ull) return false;
+  }
   return false;
 }
 
