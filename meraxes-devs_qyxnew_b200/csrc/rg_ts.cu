@@ -25,6 +25,7 @@
 
 #include "rg_internal.h"
 #include "rg_pass.cuh"
+#include "rg_tma.cuh"
 #include "rg_xray.h"
 
 namespace rg {
@@ -370,39 +371,32 @@ struct TsZ {
   static constexpr int Q = pow2_div(N, cmax(256 / T, 4));   // rows per block
   static constexpr int NTH = T * Q;
   static constexpr int MINB = NTH >= 512 ? 1 : 512 / NTH;   // 2 blocks of 256: at most 128 registers
-  static constexpr size_t tile_elems() { return (size_t)2 * (N / 2 + 1) * Q; }   // two shells' rows
+  static constexpr int NZ = N / 2 + 1;
+  // kz rows per tensor box (at most 256): one box, or for N = 512 two of (NZ + 1) / 2 rows at kz 0
+  // and NZ - KZB that overlap in one row, so the second lands on a 128-byte boundary
+  static constexpr int KZB = NZ <= 256 ? NZ : (NZ + 1) / 2;
+  static constexpr int NBOX = NZ <= 256 ? 1 : 2;
+  static constexpr int TS = round_up(NZ * Q, 16);            // one shell's rows, a 128-byte multiple
+  static constexpr size_t tile_elems() { return (size_t)2 * TS; }   // two shells' rows
+  static constexpr uint32_t SHELL_TX = (uint32_t)(NBOX * KZB * Q * sizeof(cf));
   static constexpr int STAGES = 3;           // tiles in flight: units u + 1 and u + 2 load during u
   static constexpr size_t smem() {
-    return sizeof(cf) * (N + (size_t)line_buf_r0<N, R0, Q>() + STAGES * tile_elems());
+    return 128 + sizeof(cf) * (STAGES * tile_elems() + (size_t)line_buf_r0<N, R0, Q>() + N) +
+           sizeof(uint64_t) * STAGES;
   }
+  static_assert(Q % 2 == 0 && 2 * Q <= 256, "tensor box of 2Q floats, x a 16-byte multiple");
+  static_assert(NBOX == 1 || ((NZ - KZB) * Q * sizeof(cf)) % 128 == 0, "second box off a 128-byte boundary");
 };
 
-// the Hermitian halves of rows [y0, y0 + Q) of plane x of two shells' grids a, b (b may be null:
-// zeros) as a shared tile tile[s][k][j] = (s ? b : a)[k][x][y0 + j], copied by the whole block
-template <int N, int Q>
-__device__ __forceinline__ void ts_tile_issue(cf* tile, const cf* __restrict__ a, const cf* __restrict__ b, int x,
-                                              int y0, int nth) {
-  constexpr int NZ = N / 2 + 1, C = NZ * Q / 2;   // 16-byte chunks per shell
-  for (int c = threadIdx.x; c < 2 * C; c += nth) {
-    const int s = c / C, cc = c % C;
-    const int k = cc / (Q / 2), j = 2 * (cc % (Q / 2));
-    cf* dst = tile + ((size_t)s * NZ + k) * Q + j;
-    const cf* g = s ? b : a;
-    if (g) {
-      cp_async16(dst, g + ((size_t)k * N + x) * N + y0 + j);
-    } else {
-      dst[0] = cf{0.f, 0.f};
-      dst[1] = cf{0.f, 0.f};
-    }
-  }
-}
+constexpr int TS_TMA_WAIT_LIMIT = 1 << 22;   // polls of an mbarrier before a wait gives up
 
-// complex line of row q of the two shells in a tile (shell a real part, shell b imaginary part)
+// complex line of row q of the two shells in a tile (shell a real part, shell b imaginary part);
+// the tile holds tile[s][k][j] = (s ? b : a)[k][x][y0 + j], shell b at TS
 template <int N, int Q>
 __device__ __forceinline__ cf ts_tile_input(const cf* tile, int q, int p) {
-  constexpr int NZ = N / 2 + 1;
+  constexpr int TS = TsZ<N>::TS;
   const int k = p <= N / 2 ? p : N - p;
-  const cf A = tile[k * Q + q], B = tile[(NZ + k) * Q + q];
+  const cf A = tile[k * Q + q], B = tile[TS + k * Q + q];
   if (p == 0 || p == N / 2) return cf{A.x, B.x};
   if (p < N / 2) return cf{A.x - B.y, A.y + B.x};
   return cf{A.x + B.y, B.x - A.y};
@@ -410,23 +404,31 @@ __device__ __forceinline__ cf ts_tile_input(const cf* tile, int q, int p) {
 
 // G grids per shell: 0 sfr, 1 X-ray, 2 and 3 the AGN bands in use (their per-cell heating
 // terms also go to agn_heat, for the AGN heating averages)
+// The shells' Hermitian column tiles arrive by tensor loads (the spectra as the tensor `tmap`:
+// floats y innermost, then x, then kz of spectrum r G + g at (r G + g)(N/2 + 1) + kz), STAGES
+// tiles in flight, one mbarrier each.
 template <int N, int G>
 __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
-    k_ts_zsum(const cf* __restrict__ work, size_t stride, const cf* __restrict__ g_tw,
+    k_ts_zsum(const __grid_constant__ CUtensorMap tmap, const cf* __restrict__ g_tw,
               const TsShellCoef* __restrict__ gco, TsZev zv, const float* __restrict__ xe_prev,
-              float4* __restrict__ sums, float2* __restrict__ agn_heat) {
+              float4* __restrict__ sums, float2* __restrict__ agn_heat, uint32_t* err) {
   using Z = TsZ<N>;
   using PL = typename Z::PL;
-  constexpr int Q = Z::Q, V = Z::V;
+  constexpr int Q = Z::Q, V = Z::V, NZ = Z::NZ, KZB = Z::KZB;
   constexpr int PADW = 2 * (N / 2 + 1);
-  extern __shared__ __align__(16) unsigned char smem_raw[];  // 16-byte aligned for cp.async
-  cf* smem = reinterpret_cast<cf*>(smem_raw);
-  cf* s_tw = smem;
-  cf* xbuf = smem + N;
-  cf* tiles = xbuf + line_buf_r0<N, Z::R0, Q>();
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* sm = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  cf* tiles = reinterpret_cast<cf*>(sm);
+  cf* xbuf = tiles + Z::STAGES * Z::tile_elems();
+  cf* s_tw = xbuf + line_buf_r0<N, Z::R0, Q>();
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
   __shared__ TsShellCoef sc[2];
   const int x = blockIdx.y, y = blockIdx.x * Q + threadIdx.x % Q;
   const int t = threadIdx.x / Q;
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < Z::STAGES; ++b) mbar_init(&bars[b], 1);
+    mbar_init_fence();
+  }
   load_twiddles_p<PL>(s_tw, g_tw);
   const size_t row = (size_t)x * N + y;
   // this thread's cells: z = last_pos(t, s); x_e interpolation node and offset
@@ -454,11 +456,12 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
     lopack |= (uint32_t)m << (4 * sl);
     dxe[sl] = (float)(xc - (double)xm);
   }
-  // all of this thread's cells on one x_e node (the common case early in reionization): the
-  // coefficient reads leave the per-cell loops
+  // every thread's cells each on one x_e node of their own (the common case early in
+  // reionization): the coefficient reads leave the per-cell loops.  The choice is the block's, as
+  // both paths run transforms with block barriers.
   static_assert(V == 8, "eight x_e node indices in one 32-bit word");
   const uint32_t lo0 = lopack & 15u;
-  const bool uni = lopack == lo0 * 0x11111111u;
+  const bool uni = __syncthreads_and(lopack == lo0 * 0x11111111u) != 0;
   float a_heat[V], a_ion[V], a_lya[V], a_star[V];
   float a_agn0[G > 2 ? V : 1], a_agn1[G > 3 ? V : 1];
 #pragma unroll
@@ -469,19 +472,36 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
   for (int sl = 0; sl < (G > 3 ? V : 1); ++sl) a_agn1[sl] = 0.f;
   auto addr = [&](int p) { return line_addr_r0<Z::R0, Q>(p, threadIdx.x % Q); };
   // units u = G (r / 2) + g: the pair of shells (r, r + 1), grid g; the tiles of units u + 1 and
-  // u + 2 are copied while unit u is transformed (three buffers)
+  // u + 2 load while unit u is transformed (three buffers).  A pair without its second shell (an
+  // odd count) gets zeros there, written by the block.
   constexpr int S = Z::STAGES;
   const int y0 = blockIdx.x * Q, q = threadIdx.x % Q;
-  auto unit_src = [&](int u, int which) -> const cf* {
-    const int r = 2 * (u / G) + which, g = u % G;
-    return r < zv.nS ? work + ((size_t)r * G + g) * stride : nullptr;
-  };
   const int nunits = G * ((zv.nS + 1) / 2);
+  auto has_b = [&](int u) { return 2 * (u / G) + 1 < zv.nS; };
+  // thread 0: tensor loads of unit u into its buffer
+  auto issue = [&](int u) {
+    const int b = u % S;
+    const bool two = has_b(u);
+    mbar_arrive_expect_tx(&bars[b], (two ? 2u : 1u) * Z::SHELL_TX);
+    for (int sh = 0; sh < (two ? 2 : 1); ++sh) {
+      const int spec = (2 * (u / G) + sh) * G + u % G;
 #pragma unroll
-  for (int u = 0; u < S - 1; ++u) {
-    if (u < nunits) ts_tile_issue<N, Q>(tiles + u * Z::tile_elems(), unit_src(u, 0), unit_src(u, 1), x, y0, Z::NTH);
-    cp_async_commit();
-  }
+      for (int k = 0; k < Z::NBOX; ++k) {
+        const int k0 = k ? NZ - KZB : 0;
+        tma_load_3d(tiles + b * Z::tile_elems() + sh * Z::TS + k0 * Q, &tmap, 2 * y0, x, spec * NZ + k0, &bars[b]);
+      }
+    }
+  };
+  auto zero_b = [&](int u) {
+    cf* tb = tiles + (u % S) * Z::tile_elems() + Z::TS;
+    for (int i = threadIdx.x; i < NZ * Q; i += Z::NTH) tb[i] = cf{0.f, 0.f};
+  };
+  __syncthreads();   // barriers initialised
+  if (threadIdx.x == 0)
+    for (int u = 0; u < S - 1 && u < nunits; ++u) issue(u);
+  for (int u = 0; u < S - 1 && u < nunits; ++u)
+    if (!has_b(u)) zero_b(u);
+  bool waited = true;
   // an AGN unit j: clamped at 0 (ComputeTs.c:615-630), its own band tables
   auto agn_unit = [&](const cf* tile, int j, float (&ah)[G > 2 ? V : 1]) {
     line_fft_p<PL, true>(
@@ -516,11 +536,11 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
       }
     }
     // buffer (u + 2) % 3 was consumed by unit u - 1 (the barrier at the end of its iteration)
-    if (u + S - 1 < nunits)
-      ts_tile_issue<N, Q>(tiles + ((u + S - 1) % S) * Z::tile_elems(), unit_src(u + S - 1, 0),
-                          unit_src(u + S - 1, 1), x, y0, Z::NTH);
-    cp_async_commit();
-    cp_async_wait<S - 1>();   // every group but the last S - 1: unit u's tile has landed
+    if (u + S - 1 < nunits) {
+      if (threadIdx.x == 0) issue(u + S - 1);
+      if (!has_b(u + S - 1)) zero_b(u + S - 1);
+    }
+    if (!mbar_wait(&bars[u % S], (uint32_t)((u / S) & 1), TS_TMA_WAIT_LIMIT)) waited = false;
     __syncthreads();  // unit u's tile (and the pair's coefficients) are visible to every thread
     const cf* tile = tiles + (u % S) * Z::tile_elems();
     if (g == 0) {
@@ -570,8 +590,11 @@ __global__ void __launch_bounds__(TsZ<N>::NTH, TsZ<N>::MINB)
         agn_unit(tile, 1, a_agn1);
       }
     }
-    __syncthreads();  // the tile is consumed before unit u + 3 refills it
+    // the tile is consumed (generic reads ordered before the tensor load that refills it)
+    fence_proxy_async_smem();
+    __syncthreads();
   }
+  if (!waited && threadIdx.x % 32 == 0) atomicExch(err, 1u);
 #pragma unroll
   for (int sl = 0; sl < V; ++sl) {
     const size_t ic = row * N + last_pos<PL>(t, sl);
@@ -774,10 +797,18 @@ static int launch_ts_zsum_g(rg_context* ctx, const cf* work, size_t stride, cons
   if (rc) return rc;
   using Z = TsZ<N>;
   const double n3 = (double)N * N * N, nzc = (double)(N / 2 + 1) * N * N;
+  if (stride != (size_t)Z::NZ * N * N) return set_error(ctx, RG_EINVAL, "Ts z pass: shell spectra must be contiguous");
+  // every shell's G spectra (S[kz][x][y], one after another) as a 3-D float tensor
+  CUtensorMap tmap;
+  const uint64_t dims[3] = {2ull * N, (uint64_t)N, (uint64_t)Z::NZ * zv.nS * G};
+  const uint64_t strides[2] = {8ull * N, 8ull * N * N};
+  const uint32_t box[3] = {2u * Z::Q, 1u, (uint32_t)Z::KZB};
+  const int mrc = tma_map_3d(&tmap, work, dims, strides, box);
+  if (mrc != 0) return set_error(ctx, RG_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(mrc) + ")");
   const size_t smz = Z::smem();
   RG_CUDA_TRY(ctx, cudaFuncSetAttribute(k_ts_zsum<N, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
   prof_begin(ctx, "ts_z_c2r_sums", st);
-  k_ts_zsum<N, G><<<dim3(N / Z::Q, N), Z::NTH, smz, st>>>(work, stride, tw, d_co, zv, xe_prev, sums, agn_heat);
+  k_ts_zsum<N, G><<<dim3(N / Z::Q, N), Z::NTH, smz, st>>>(tmap, tw, d_co, zv, xe_prev, sums, agn_heat, ctx->xy_ctrl);
   // Hermitian halves of the G grids of every shell, x_e read, four float sums (and the AGN
   // heating pair) written
   prof_end(ctx, zv.nS * G * 8.0 * nzc + 4.0 * n3 + 16.0 * n3 + (G > 2 ? 8.0 * n3 : 0.0), st);
@@ -1166,10 +1197,12 @@ int ts_snapshot(rg_context* ctx, const rg_params* p, const rg_snapshot* s, const
     zv.nS = nS;
     if ((rc = ensure_device(ctx, &ctx->ts_sums, &ctx->ts_sums_elems, n3))) return rc;
     if (nagn && (rc = ensure_device(ctx, &ctx->ts_agn, &ctx->ts_agn_elems, n3))) return rc;
+    if ((rc = xy_ctrl_reset(ctx, 0, st))) return rc;   // the error word of the tile waits
     if ((rc = ts_zsum(ctx, N, ctx->work, nc, G, d_co, zv, g->x_e_box_prev, ctx->ts_sums, nagn ? ctx->ts_agn : nullptr,
                       st)))
       return rc;
     RG_CUDA_TRY(ctx, cudaStreamSynchronize(st));  // hco outlives the copy
+    if ((rc = xy_ctrl_check(ctx, st))) return rc;
   }
 
   TsEvolve e;
