@@ -127,10 +127,11 @@ __host__ __device__ constexpr int line_buf_r0() {
 
 // ---------------------------------------------------------------------------
 
-// the forward z pass's launch shape: QF row pairs per block, one line of T threads each
+// the forward z pass's launch shape: QF row pairs per block, one line of T threads each (the
+// default plans: at 512 the 32-thread plan measured slower here, 6.9 against 5.6 ms a snapshot)
 template <int N>
 struct ZFCfg {
-  using PL = PlanW<N>;
+  using PL = Plan<N>;
   static constexpr int T = PL::T;
   static constexpr int QF = pow2_div(N / 2, cmax(256 / T, 1));
   static constexpr int NTH = T * QF;
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(ZFCfg<N>::NTH, RG_MINB(ZFCfg<N>::NTH))
   load_twiddles_p<PL>(s_tw, g_tw);
   __syncthreads();
   const float* r0 = src + ((size_t)x * N + y0 + 2 * q) * PADW;
-  line_fft_p<PL, false, true>(   // warp barriers: a line's threads are one warp's lanes, its rows its own
+  line_fft_p<PL, false, (T <= 32)>(   // warp barriers when a line fits a warp (its rows are its own)
       t, xbuf, s_tw, [&](int p, int) { return cf{__ldg(r0 + p), __ldg(r0 + PADW + p)}; },
       [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v, int) { zbuf[pos_addr<N>(q, p)] = v; });
   __syncthreads();

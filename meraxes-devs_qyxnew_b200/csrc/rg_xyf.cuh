@@ -86,43 +86,24 @@ __device__ __forceinline__ void xy_wait(const XYSched& s, int job) {
 // The fused pass's plans (PlanW): at 512, 8 x 16 x 4 over 32 threads a line measured faster than
 // 8 x 8 x 8 over 64 (77.2 against 81.3 ms for the 61 radii of a 512^3 snapshot; 16 x 16 x 2 took
 // 78.5 ms, and 16 columns an item instead of 8 took 85-87 ms), and its Y lines are warp-local.
-//
-// Every line, X column or Y row, is transformed by T <= 32 consecutive lanes of one warp (thread
-// t = threadIdx % T of line threadIdx / T) through its own row of the exchange buffer, so the
-// transforms synchronise per warp.  An X tile arrives as B / 2 column-pair tiles [x][2 columns]
-// (tensor boxes 16 bytes wide), in which a column's values sit 16 bytes apart; the transform's
-// outputs go back to the column's own slots and leave the block as rows of B columns.
 template <int N>
 struct XYF {
   using PL = PlanW<N>;
   static constexpr int T = PL::T;
   static constexpr int V = N / T;
   static constexpr int B = Cfg<N>::BX;   // columns per X item, lines per Y item
-  static constexpr int NP = B / 2;       // column pairs per X tile
   static constexpr int MINB = N != 512 ? x_pass_minb<N>() : 2;
   static constexpr int NTH = T * B;
   static constexpr int M = N / B;
   static constexpr int XROWS = N <= 256 ? N : N / 2;   // x rows per tensor box (box dimensions <= 256)
   static constexpr int NXB = N / XROWS;
-  static constexpr int TB = N * B;                     // a tile buffer: NP pair tiles of 2N values
-  static constexpr int PX = round_up(N + N / 16, 16) + 4;   // exchange row pitch, 4 mod 16 (banks)
+  // a buffer: an X tile [x][B columns], then its exchange buffer; or a Y item's exchange buffer
+  static constexpr int TB = round_up(cmax(cmax(line_buf_r0<N, PL::R[0], B>(), B * Cfg<N>::PITCH_P), N * B), 16);
   static constexpr int ZB = 2;
   static constexpr uint32_t TX = (uint32_t)(N * B * sizeof(cf));
-  static constexpr size_t smem() {
-    return 128 + sizeof(cf) * ((size_t)ZB * TB + (size_t)B * PX + N) + sizeof(uint64_t) * ZB;
-  }
-  static_assert(B % 2 == 0 && (2 * N * sizeof(cf)) % 128 == 0 && (XROWS * 2 * sizeof(cf)) % 128 == 0,
-                "pair tiles off 128-byte boundaries");
-  static_assert(T <= 32 && 32 % T == 0, "a line's threads within one warp");
+  static constexpr size_t smem() { return 128 + sizeof(cf) * ((size_t)ZB * TB + N) + sizeof(uint64_t) * ZB; }
+  static_assert((XROWS * B * sizeof(cf)) % 128 == 0, "second x box off a 128-byte boundary");
 };
-
-// exchange-buffer index of position p of line b (one pad slot every 16 positions, or an XOR of
-// the position's low bits for 192/384/512, against the stride-R patterns of the first stages)
-template <int N>
-__device__ __forceinline__ int xy_addr(int b, int p) {
-  if constexpr (N == 192 || N == 384 || N == 512) return b * XYF<N>::PX + (p ^ ((p >> 3) & 15));
-  return b * XYF<N>::PX + p + (p >> 4);
-}
 
 __device__ __forceinline__ cf ldcg_cf(const cf* p) {
   const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
@@ -154,8 +135,7 @@ __global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
   unsigned char* sm = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   cf* bufs = reinterpret_cast<cf*>(sm);
   cf* s_tw = bufs + F::ZB * TB;
-  cf* xbuf = s_tw + N;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(xbuf + B * F::PX);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_tw + N);
   __shared__ int s_item[2];
   __shared__ int s_pref[2];   // the next item's first tile is in flight
   if (threadIdx.x == 0) {
@@ -178,11 +158,8 @@ __global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
     const int kz = job / sch.nr;
     mbar_arrive_expect_tx(&bars[b], F::TX);
 #pragma unroll
-    for (int q = 0; q < F::NP; ++q)
-#pragma unroll
-      for (int xb = 0; xb < F::NXB; ++xb)
-        tma_load_3d(bufs + b * TB + q * 2 * N + xb * F::XROWS * 2, &smap, 2 * (k * B + 2 * q), xb * F::XROWS,
-                    g * NZ + kz, &bars[b]);
+    for (int xb = 0; xb < F::NXB; ++xb)
+      tma_load_3d(bufs + b * TB + xb * F::XROWS * B, &smap, 2 * k * B, xb * F::XROWS, g * NZ + kz, &bars[b]);
   };
   auto is_x_item = [&](int itm) {
     if (itm >= sch.total) return false;
@@ -207,8 +184,9 @@ __global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
     const size_t plane = (size_t)kz * N * N;
     int next_pref = 0;
     if (!is_y) {
-      const int t = threadIdx.x % T, bcol = threadIdx.x / T;
+      const int bcol = threadIdx.x % B, t = threadIdx.x / B;
       const int y = k * B + bcol;
+      const size_t col = plane + y;
       float wv[V];
 #pragma unroll
       for (int sl = 0; sl < V; ++sl) wv[sl] = 1.f;
@@ -238,25 +216,17 @@ __global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
         }
         if (!mbar_wait(&bars[b], (xu >> 1) & 1u, 1 << 22)) waited = false;
         cf* tile = bufs + b * TB;
-        // this column's slots of its pair tile: inputs, then (after the warp's exchanges) outputs
-        cf* mine = tile + (bcol >> 1) * 2 * N + (bcol & 1);
-        line_fft_p<PL, true, true>(
-            t, xbuf, s_tw,
+        cf* dst = op.out(r, g);
+        line_fft_p<PL, true>(
+            t, tile, s_tw,
             [&](int p, int sl) {
-              const cf v = mine[2 * p];
+              const cf v = tile[p * B + bcol];
               return cf{v.x * wv[sl], v.y * wv[sl]};
             },
-            [&](int p) { return xy_addr<N>(bcol, p); }, [&](int p, cf v, int) { mine[2 * p] = v; });
-        __syncthreads();   // every column's outputs are in the tile
-        // rows of the B columns, one column pair (16 bytes) a thread
-        cf* dst = op.out(r, g) + plane + (size_t)k * B;
-        for (int i = threadIdx.x; i < N * F::NP; i += F::NTH) {
-          const int q = i % F::NP, p = i / F::NP;
-          const float4 v = *reinterpret_cast<const float4*>(tile + q * 2 * N + 2 * p);
-          *reinterpret_cast<float4*>(dst + (size_t)p * N + 2 * q) = v;
-        }
+            [&](int p) { return line_addr_r0<PL::R[0], B>(p, bcol); },
+            [&](int p, cf v, int) { dst[col + (size_t)p * N] = v; });
         fence_proxy_async_smem();
-        __syncthreads();   // the tile and the exchange rows are free: its buffer may be refilled
+        __syncthreads();   // every store of the unit is issued; its buffer may be refilled
       }
       if (threadIdx.x == 0 && sch.signal) xy_signal(sch.done + job);
     } else {
@@ -267,10 +237,11 @@ __global__ void __launch_bounds__(XYF<N>::NTH, XYF<N>::MINB)
       // a line's T <= 32 threads are consecutive lanes of one warp, its exchange rows its own
       for (int g = 0; g < ng; ++g) {
         cf* line = op.out(r, g) + row;
-        line_fft_p<PL, true, true>(
-            t, xbuf, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return xy_addr<N>(b, p); },
+        line_fft_p<PL, true, (T <= 32)>(
+            t, bufs, s_tw, [&](int p, int) { return ldcg_cf(line + p); }, [&](int p) { return pos_addr<N>(b, p); },
             [&](int p, cf v, int) { line[p] = v; });
       }
+      fence_proxy_async_smem();   // the exchange buffer is a tile buffer of later X items
     }
     if (threadIdx.x == 0) {
       s_item[(it + 1) & 1] = nxt;
@@ -296,7 +267,7 @@ int launch_xy_fused(rg_context* ctx, const Op& op, const cf* spec, int nspec, in
   CUtensorMap smap;
   const uint64_t dims[3] = {2ull * N, (uint64_t)N, (uint64_t)Cfg<N>::NZ * nspec};
   const uint64_t strides[2] = {8ull * N, 8ull * N * N};
-  const uint32_t box[3] = {4u, (uint32_t)F::XROWS, 1u};   // one column pair (16 bytes) of XROWS rows
+  const uint32_t box[3] = {2u * F::B, (uint32_t)F::XROWS, 1u};
   const int mrc = tma_map_3d(&smap, spec, dims, strides, box);
   if (mrc != 0) return set_error(ctx, RG_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(mrc) + ")");
   const int J = Cfg<N>::NZ * nr;
