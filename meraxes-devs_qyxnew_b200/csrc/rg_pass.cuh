@@ -135,7 +135,11 @@ struct ZFCfg {
   static constexpr int T = PL::T;
   static constexpr int QF = pow2_div(N / 2, cmax(256 / T, 1));
   static constexpr int NTH = T * QF;
-  static constexpr size_t smem() { return sizeof(cf) * (N + 2 * (size_t)QF * Cfg<N>::PITCH_P); }
+  // the split reads rows qq of the transformed pairs at KN kz values a warp: a row pitch of KN mod
+  // 16 values puts the warp's (row, kz) reads on distinct banks
+  static constexpr int KN = 2 * QF >= 32 ? 1 : 32 / (2 * QF);
+  static constexpr int ZP = round_up(Cfg<N>::PITCH_P, 16) + KN;
+  static constexpr size_t smem() { return sizeof(cf) * (N + (size_t)QF * (Cfg<N>::PITCH_P + ZP)); }
 };
 
 template <int N>
@@ -155,16 +159,18 @@ __global__ void __launch_bounds__(ZFCfg<N>::NTH, RG_MINB(ZFCfg<N>::NTH))
   load_twiddles_p<PL>(s_tw, g_tw);
   __syncthreads();
   const float* r0 = src + ((size_t)x * N + y0 + 2 * q) * PADW;
+  constexpr int ZP = ZFCfg<N>::ZP;
+  auto zpos = [&](int qq, int p) { return qq * ZP + pos_addr<N>(0, p); };
   line_fft_p<PL, false, (T <= 32)>(   // warp barriers when a line fits a warp (its rows are its own)
       t, xbuf, s_tw, [&](int p, int) { return cf{__ldg(r0 + p), __ldg(r0 + PADW + p)}; },
-      [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v, int) { zbuf[pos_addr<N>(q, p)] = v; });
+      [&](int p) { return pos_addr<N>(q, p); }, [&](int p, cf v, int) { zbuf[zpos(q, p)] = v; });
   __syncthreads();
   // split Z = X(y) + i X(y+1) and store S[k][x][y0 .. y0 + 2Q)
   for (int i = threadIdx.x; i < NZ * 2 * Q; i += T * Q) {
     const int yy = i % (2 * Q), k = i / (2 * Q);
     const int qq = yy >> 1;
-    const cf zk = zbuf[pos_addr<N>(qq, k)];
-    const cf zn = zbuf[pos_addr<N>(qq, (N - k) % N)];
+    const cf zk = zbuf[zpos(qq, k)];
+    const cf zn = zbuf[zpos(qq, (N - k) % N)];
     cf out;
     if ((yy & 1) == 0) {
       out = cf{0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y)};  // (Z[k] + conj Z[N-k]) / 2
