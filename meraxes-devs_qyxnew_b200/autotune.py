@@ -34,13 +34,18 @@ def load(path: str = CACHE) -> dict:
         return {}
 
 
-def store(entries: dict, path: str = CACHE) -> None:
+def store(entries: dict, path: str = CACHE) -> bool:
+    """Merge entries into the cache; False (nothing kept) where the file cannot be written."""
     cur = load(path)
     cur.update(entries)
     tmp = path + ".tmp"
-    with open(tmp, "w") as f:
-        json.dump(cur, f, indent=1, sort_keys=True)
-    os.replace(tmp, path)
+    try:
+        with open(tmp, "w") as f:
+            json.dump(cur, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        return False
+    return True
 
 
 def candidates(units: int) -> list[tuple[int, int]]:

@@ -33,3 +33,9 @@ def test_tune_picks_the_fastest_shape_and_caches_it(tmp_path):
     assert len(ran) == n
     autotune.store({"other": {"radius_batch": 4, "per_call": 1}}, path)
     assert key in autotune.load(path) and "other" in autotune.load(path)
+
+
+def test_store_into_an_unwritable_place_keeps_nothing(tmp_path):
+    path = str(tmp_path / "no_such_dir" / "cache.json")
+    assert autotune.store({"k": {"radius_batch": 8, "per_call": 1}}, path) is False
+    assert autotune.load(path) == {}
