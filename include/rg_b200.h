@@ -346,7 +346,7 @@ int rg_debug_set_wait_limits(rg_context* ctx, int xy_poll_limit, int xy_signal, 
      RG_DFT_FP32       the FP32 register-resident transform the step's passes use;
      RG_DFT_TC_BF16X3  the split-BF16 tensor-core form: 256 = 16 x 16, each radix-16 stage a
                        tcgen05 matrix product of hi/lo BF16 operands (three products) with FP32
-                       accumulation in tensor memory, about 5e-6 relative error per pass.
+                       accumulation in tensor memory, about 4.4e-6 relative error per pass.
    spec: device pointer, 16-byte aligned, n_grids * 129 * 256 * 256 complex64.  Both forms
    compute what the y stage of FFTW's 3-D transforms computes (find_HII_bubbles.c:351-370,
    ComputeTs.c:480-581); this entry point exists to compare them.  ReionGridDim other than 256

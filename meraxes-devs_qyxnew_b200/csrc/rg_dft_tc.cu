@@ -10,9 +10,10 @@
 // outputs: the 32 x 32 real form of the DFT-16 matrix.  A and B are each split into BF16 hi and
 // lo parts (v = hi + lo to about 2^-17 relative) and D = Ahi Bhi + Alo Bhi + Ahi Blo is
 // accumulated in FP32 in tensor memory by tcgen05.mma (kind::f16, M = 128, N = 32, K = 16 per
-// instruction, both operands K-major in shared memory without swizzle); the dropped Alo Blo term
-// and the splits leave about 4e-6 relative error per stage.  One thread (TMEM lane) per matrix
-// row reads its 32 accumulators back with tcgen05.ld.
+// instruction, both operands K-major in shared memory without swizzle).  The two-part operands
+// (about 16 significant bits) leave about 4e-6 relative error per pass; the dropped Alo Blo term
+// adds little.  One thread (TMEM lane) per matrix row reads its 32 accumulators back with
+// tcgen05.ld.
 //
 // It replaces nothing of the reference's code by itself: the reference transforms with FFTW
 // (find_HII_bubbles.c:351-370, ComputeTs.c:480-581), whose y stage both forms implement.  It is
