@@ -91,3 +91,18 @@ def test_split_bf16_inverse_pass_matches_fp64():
     x = (rng.standard_normal((128, 256)) + 1j * rng.standard_normal((128, 256))).astype(np.complex64)
     want = np.fft.ifft(x.astype(np.complex128), axis=1) * 256
     assert rel_l2(tc_pass(x, sign=+1), want) < 1e-5
+
+
+def test_split_bf16_errors_accumulate_over_passes():
+    """A forward and inverse 2-D transform (four passes) by this arithmetic returns the input to
+    about 9e-6: a 3-D forward and inverse (six passes, every filtered field of the step) would be
+    above the 1e-5 gates."""
+    rng = np.random.default_rng(5)
+    x = (rng.standard_normal((256, 256)) + 1j * rng.standard_normal((256, 256))).astype(np.complex64)
+    y = tc_pass(x)
+    y = tc_pass(y.T.astype(np.complex64)).T
+    z = tc_pass(y.T.astype(np.complex64), sign=+1).T
+    z = tc_pass(z.astype(np.complex64), sign=+1)
+    e = rel_l2(z / 256 ** 2, x.astype(np.complex128))
+    assert 6e-6 < e < 1.2e-5, e
+    assert e * np.sqrt(6 / 4) > 1e-5
