@@ -3,6 +3,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -84,3 +85,22 @@ PARITY_ROWS: list = []
 
 def record(config: str, output: str, measure: str, value: float, gate: str):
     PARITY_ROWS.append((config, output, measure, float(value), gate))
+
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(name: str):
+    """Outputs of the reference's own compiled step for a test case (tests/golden/make_golden.py),
+    as ref_lib.run_step returns them (grids, and the box averages under "scalars"); None when the
+    file is absent."""
+    path = os.path.join(GOLDEN_DIR, name + ".npz")
+    if not os.path.exists(path):
+        return None
+    with np.load(path) as f:
+        d = {k: f[k] for k in f.files}
+    scal = {"volume_weighted_global_xH": float(d.pop("mean_xH"))}
+    if "mean_Tb" in d:
+        scal["volume_ave_Tb"] = float(d.pop("mean_Tb"))
+    d["scalars"] = scal
+    return d

@@ -37,7 +37,7 @@ import reion_oracle as ro
 import rg_b200 as rg
 import ts_oracle as to
 import workloads as wl
-from helpers import DeviceGrids, install_recfast, oracle_params, record, rel_l2
+from helpers import DeviceGrids, golden, install_recfast, oracle_params, record, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -378,16 +378,18 @@ def _ref_lib():
 def test_c0_64_find_hii_against_reference_code(ftype):
     """c0_64's grid, box and redshift at an efficiency that ionises part of the box: the GPU's
     find_HII_bubbles against the reference's compiled _find_HII_bubbles on the same inputs (the
-    reference computes in float, so the gates are the FP64 ones with the FP64 oracle's margins)."""
-    ref_lib = _ref_lib()
+    reference computes in float, so the gates are the FP64 ones with the FP64 oracle's margins).
+    The reference's outputs are its golden files (tests/golden), or a run of oracle/_ref."""
     cfg = wl.CONFIGS["c0_64"]
     n = cfg.n
     src = wl.make_sources(cfg.n, cfg.box, cfg.seed, cfg.source_scale)
     p = hii_params(cfg, 4000.0, ftype)
     res, out = gpu_hii(p, n, cfg.z, src)
     zz, snap = wl.snapshot_redshifts(cfg.z)
-    ref = ref_lib.run_step(oracle_params(p), zz, snap, {"deltax": src.deltax, "stars": src.stars,
-                                                         "weighted_sfr": src.sfr})
+    ref = golden(f"c0_64_f{ftype}")
+    if ref is None:
+        ref = _ref_lib().run_step(oracle_params(p), zz, snap, {"deltax": src.deltax, "stars": src.stars,
+                                                                "weighted_sfr": src.sfr})
     diag = fp64_hii(p, cfg.z, src, numpy_oracle=True)[3]
     near = diag["min_margin"] <= 1e-4
     tag = f"c0_64 filter {ftype} eff 4000 vs reference code"
@@ -412,8 +414,8 @@ def test_c0_64_find_hii_against_reference_code(ftype):
 
 def test_step_chain_against_reference_code():
     """ComputeTs -> find_HII_bubbles -> delta_T at 32^3 on the GPU against the reference's compiled
-    _ComputeTs, _find_HII_bubbles and ComputeBrightnessTemperatureBox."""
-    ref_lib = _ref_lib()
+    _ComputeTs, _find_HII_bubbles and ComputeBrightnessTemperatureBox (its golden files, or a run
+    of oracle/_ref)."""
     n, box, z = 32, 64.0, 13.0
     zz, snap = wl.snapshot_redshifts(z)
     src = wl.make_sources(n, box, 600)
@@ -424,9 +426,11 @@ def test_step_chain_against_reference_code():
     inputs = dict(deltax=src.deltax, stars=src.stars, weighted_sfr=src.sfr, sfr=src.sfr, xray_luminosity=src.xray,
                   x_e_box_prev=ti.x_e_box_prev, Tk_box=ti.Tk_box, sfr_histories=np.stack(ti.sfr_histories),
                   xray_luminosity_histories=np.stack(ti.xray_histories))
-    ref = ref_lib.run_step(oracle_params(p), zz, snap, inputs, stages=("ts", "hii", "dT"),
-                           n_hist=len(ti.sfr_histories), stored_fcoll=ti.stored_fcoll,
-                           outputs=("x_e_box", "Tk_box", "TS_box", "xH", "delta_T"))
+    ref = golden("chain_32")
+    if ref is None:
+        ref = _ref_lib().run_step(oracle_params(p), zz, snap, inputs, stages=("ts", "hii", "dT"),
+                                  n_hist=len(ti.sfr_histories), stored_fcoll=ti.stored_fcoll,
+                                  outputs=("x_e_box", "Tk_box", "TS_box", "xH", "delta_T"))
     tag = "chain 32^3 vs reference code"
     U = wl.from_padded
     e = rel_l2(U(res["x_e_box"]), U(ref["x_e_box"].reshape(n, n, -1)))
